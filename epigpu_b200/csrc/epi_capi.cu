@@ -1,0 +1,610 @@
+// epi_capi.cu -- the C ABI of libepigpu.so (include/epigpu.h).
+//
+// Host side of the scan: device selection, genotype and trait upload, the tile schedule
+// over chromosome blocks, kernel dispatch (plain popcount form / tcgen05 tensor form),
+// hit readback and ordering. It replaces the OpenCL host code of perform_scan
+// (src/EpiOpenCL.c:1383-1627); the results file itself is written by the C host
+// (epigpu_b200/host/scan_driver.c).
+#include "epigpu.h"
+#include "epi_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+namespace epi {
+cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int remain, uint4 *planes, int Wp,
+                          uint32_t *codes, int Wc, cudaStream_t stream);
+cudaError_t launch_popc(const ScanArgs &a, int grid, cudaStream_t stream);
+int popc_tile_i();
+int popc_tile_j();
+// tensor form (scan_mma.cu)
+bool mma_available();
+int mma_tile_i();
+int mma_tile_j();
+int mma_min_nid();
+cudaError_t launch_mma(const ScanArgs &a, int grid, cudaStream_t stream);
+}  // namespace epi
+
+using epi::BlockDesc;
+using epi::DevHit;
+
+struct epi_ctx {
+    int device = -1;
+    int sm_count = 0;
+    char name[256] = {0};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // genotypes
+    int nid = 0, nsnp = 0, npack = 0, remain = 0;
+    int Wp = 0, Wc = 0, Np = 0;
+    int32_t *d_raw = nullptr;
+    size_t raw_cap = 0;
+    uint4 *d_planes = nullptr;
+    uint32_t *d_codes = nullptr;
+    size_t planes_cap = 0, codes_cap = 0;
+    // traits
+    int ntraits = 0, traits_nid = 0;
+    float *d_y = nullptr, *d_q = nullptr;
+    uint32_t *d_wmask = nullptr;
+    double *d_qc = nullptr, *d_yscale = nullptr, *d_qscale = nullptr;
+    int8_t *d_ydig = nullptr;
+    size_t traits_cap = 0, ydig_cap = 0;
+    std::vector<double> qc;
+    // scan scratch
+    DevHit *d_hits = nullptr;
+    int64_t hit_cap = 0;
+    unsigned long long *d_counters = nullptr;
+    unsigned int *d_maxf = nullptr;
+    int maxf_cap = 0;
+    BlockDesc *d_blocks = nullptr;
+    int blocks_cap = 0;
+    // last scan
+    double last_ms = 0.0;
+    int64_t last_pairs = 0;
+    int last_launches = 0;
+    std::string err;
+};
+
+static epi_status set_err(epi_ctx *ctx, epi_status s, const char *fmt, ...)
+{
+    if (ctx) {
+        char buf[1024];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        ctx->err = buf;
+    }
+    return s;
+}
+
+#define CK(call)                                                                                      \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return set_err(ctx, e_ == cudaErrorMemoryAllocation ? EPI_E_NOMEM : EPI_E_CUDA,          \
+                           "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);      \
+    } while (0)
+
+template <class T>
+static cudaError_t ensure(T **p, size_t *cap_bytes, size_t bytes)
+{
+    if (*p && *cap_bytes >= bytes) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap_bytes = 0;
+    cudaError_t e = cudaMalloc((void **)p, bytes ? bytes : 16);
+    if (e == cudaSuccess) *cap_bytes = bytes;
+    return e;
+}
+
+extern "C" {
+
+void epi_default_opts(epi_scan_opts *o)
+{
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->test = 'f';
+    o->safe = 0;
+    o->chunk = 128;
+    o->t1 = 6.5f;
+    o->t2 = 10.5f;
+    o->form = EPI_FORM_AUTO;
+    o->report_trait = 0;
+}
+
+const char *epi_strerror(epi_status s)
+{
+    switch (s) {
+    case EPI_OK: return "success";
+    case EPI_E_INVALID: return "invalid argument";
+    case EPI_E_CUDA: return "CUDA error";
+    case EPI_E_NOMEM: return "out of device memory";
+    case EPI_E_OVERFLOW: return "more hits than the output capacity";
+    case EPI_E_STATE: return "genotypes or phenotypes not loaded";
+    case EPI_E_TIMEOUT: return "device wait timed out";
+    case EPI_E_NODEVICE: return "no suitable CUDA device";
+    case EPI_E_UNSUPPORTED: return "unsupported option for this form";
+    }
+    return "unknown status";
+}
+
+const char *epi_last_error(const epi_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+epi_status epi_open(int32_t device, epi_ctx **out)
+{
+    if (!out) return EPI_E_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return EPI_E_NODEVICE;
+    if (device < 0 || device >= n) return EPI_E_NODEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return EPI_E_NODEVICE;
+    if (prop.major != 10) return EPI_E_NODEVICE;  // the library carries sm_100a code only
+    epi_ctx *ctx = new epi_ctx();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    snprintf(ctx->name, sizeof(ctx->name), "%s", prop.name);
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&ctx->d_counters, 4 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        epi_close(ctx);
+        return EPI_E_CUDA;
+    }
+    *out = ctx;
+    return EPI_OK;
+}
+
+epi_status epi_close(epi_ctx *ctx)
+{
+    if (!ctx) return EPI_OK;
+    if (ctx->device >= 0) cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    void *bufs[] = {ctx->d_raw, ctx->d_planes, ctx->d_codes, ctx->d_y, ctx->d_q, ctx->d_wmask, ctx->d_qc,
+                    ctx->d_yscale, ctx->d_qscale, ctx->d_ydig, ctx->d_hits, ctx->d_counters, ctx->d_maxf,
+                    ctx->d_blocks};
+    for (void *p : bufs)
+        if (p) cudaFree(p);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return EPI_OK;
+}
+
+epi_status epi_device_info(const epi_ctx *ctx, char *name, int32_t name_len, int32_t *sm_count)
+{
+    if (!ctx) return EPI_E_INVALID;
+    if (name && name_len > 0) snprintf(name, (size_t)name_len, "%s", ctx->name);
+    if (sm_count) *sm_count = ctx->sm_count;
+    return EPI_OK;
+}
+
+epi_status epi_load_packed(epi_ctx *ctx, const int32_t *gpack, int32_t nid, int32_t nsnp, int32_t npack,
+                           int32_t remain)
+{
+    if (!ctx) return EPI_E_INVALID;
+    if (!gpack || nid < 1 || nsnp < 1)
+        return set_err(ctx, EPI_E_INVALID, "epi_load_packed: need gpack, nid >= 1, nsnp >= 1");
+    if (npack != nid / 16 || remain != nid % 16)
+        return set_err(ctx, EPI_E_INVALID, "epi_load_packed: npack/remain (%d/%d) inconsistent with nid %d "
+                       "(src/readplink.c:1071-1072)", npack, remain, nid);
+    CK(cudaSetDevice(ctx->device));
+    const int npack1 = remain ? npack + 1 : npack;
+    const int Wp = ((nid + 31) / 32 + 3) / 4 * 4;  // multiple of 4 words = 128 individuals
+    const int Wc = 2 * Wp;
+    CK(ensure(&ctx->d_raw, &ctx->raw_cap, (size_t)nsnp * npack1 * sizeof(int32_t)));
+    CK(ensure(&ctx->d_planes, &ctx->planes_cap, (size_t)nsnp * Wp * sizeof(uint4)));
+    CK(ensure(&ctx->d_codes, &ctx->codes_cap, (size_t)nsnp * Wc * sizeof(uint32_t)));
+    CK(cudaMemcpyAsync(ctx->d_raw, gpack, (size_t)nsnp * npack1 * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(epi::launch_unpack(ctx->d_raw, nsnp, nid, npack, remain, ctx->d_planes, Wp, ctx->d_codes, Wc, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->traits_nid != nid) ctx->ntraits = 0;  // traits no longer match
+    ctx->nid = nid;
+    ctx->nsnp = nsnp;
+    ctx->npack = npack;
+    ctx->remain = remain;
+    ctx->Wp = Wp;
+    ctx->Wc = Wc;
+    ctx->Np = 32 * Wp;
+    return EPI_OK;
+}
+
+epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntraits, const uint8_t *valid)
+{
+    if (!ctx) return EPI_E_INVALID;
+    if (!y || nid < 1 || ntraits < 1) return set_err(ctx, EPI_E_INVALID, "epi_set_traits: bad arguments");
+    if (ctx->nid == 0) return set_err(ctx, EPI_E_STATE, "epi_set_traits: load genotypes first");
+    if (nid != ctx->nid)
+        return set_err(ctx, EPI_E_INVALID, "epi_set_traits: %d individuals, genotypes have %d", nid, ctx->nid);
+    CK(cudaSetDevice(ctx->device));
+    const int Np = ctx->Np, Wp = ctx->Wp;
+    std::vector<float> hy((size_t)ntraits * Np, 0.0f), hq((size_t)ntraits * Np, 0.0f);
+    std::vector<uint32_t> hw((size_t)ntraits * Wp, 0u);
+    ctx->qc.assign(ntraits, 0.0);
+    for (int t = 0; t < ntraits; ++t) {
+        const float *yt = y + (size_t)t * nid;
+        const uint8_t *vt = valid ? valid + (size_t)t * nid : nullptr;
+        double sum = 0.0;
+        long long nv = 0;
+        for (int k = 0; k < nid; ++k) {
+            const bool ok = vt ? vt[k] != 0 : yt[k] != -9.0f;
+            if (ok) {
+                sum += (double)yt[k];
+                ++nv;
+                hw[(size_t)t * Wp + k / 32] |= 1u << (k % 32);
+            }
+        }
+        const double mu = nv ? sum / (double)nv : 0.0;
+        double s2 = 0.0;
+        for (int k = 0; k < nid; ++k) {
+            if (hw[(size_t)t * Wp + k / 32] >> (k % 32) & 1u) {
+                const float yc = (float)((double)yt[k] - mu);
+                hy[(size_t)t * Np + k] = yc;
+                s2 += (double)yc * (double)yc;
+            }
+        }
+        const double c = nv ? s2 / (double)nv : 0.0;
+        ctx->qc[t] = c;
+        for (int k = 0; k < nid; ++k) {
+            if (hw[(size_t)t * Wp + k / 32] >> (k % 32) & 1u) {
+                const double yc = hy[(size_t)t * Np + k];
+                hq[(size_t)t * Np + k] = (float)(yc * yc - c);
+            }
+        }
+    }
+    size_t need = (size_t)ntraits * Np * sizeof(float);
+    size_t cap_y = ctx->traits_cap, cap_q = ctx->traits_cap;
+    CK(ensure(&ctx->d_y, &cap_y, need));
+    CK(ensure(&ctx->d_q, &cap_q, need));
+    ctx->traits_cap = std::min(cap_y, cap_q);
+    size_t cw = 0, cq = 0;
+    if (ctx->d_wmask) cudaFree(ctx->d_wmask);
+    if (ctx->d_qc) cudaFree(ctx->d_qc);
+    ctx->d_wmask = nullptr;
+    ctx->d_qc = nullptr;
+    CK(ensure(&ctx->d_wmask, &cw, (size_t)ntraits * Wp * sizeof(uint32_t)));
+    CK(ensure(&ctx->d_qc, &cq, (size_t)ntraits * sizeof(double)));
+    CK(cudaMemcpyAsync(ctx->d_y, hy.data(), need, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_q, hq.data(), need, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_wmask, hw.data(), hw.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_qc, ctx->qc.data(), ntraits * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->ntraits = ntraits;
+    ctx->traits_nid = nid;
+    return EPI_OK;
+}
+
+epi_status epi_set_phenotype(epi_ctx *ctx, const float *phen, int32_t nid, int32_t safe)
+{
+    if (!ctx) return EPI_E_INVALID;
+    if (!safe) return epi_set_traits(ctx, phen, nid, 1, nullptr);
+    std::vector<uint8_t> v((size_t)(nid > 0 ? nid : 0), 1);
+    return epi_set_traits(ctx, phen, nid, 1, v.data());
+}
+
+void epi_permute_phenotype(float *phen, int32_t nid, uint32_t seed)
+{
+    if (!phen) return;
+    srand(seed);
+    for (int i = nid; i > 1; i--) {
+        const int r = rand() % i;
+        const float t = phen[r];
+        phen[r] = phen[i - 1];
+        phen[i - 1] = t;
+    }
+}
+
+}  // extern "C"
+
+// number of pairs (gx, gy) of a block with start1+gx > start2+gy
+static int64_t block_pairs(const epi_block &b)
+{
+    int64_t n = 0;
+    const int64_t d = (int64_t)b.start1 - b.start2;
+    for (int64_t gx = 0; gx < b.size1; ++gx) {
+        int64_t lim = gx + d;
+        if (lim > b.size2) lim = b.size2;
+        if (lim > 0) n += lim;
+    }
+    return n;
+}
+
+namespace {
+
+struct ScanRun {
+    epi::ScanArgs args;
+    int form;
+    int64_t ntiles;
+    std::vector<BlockDesc> desc;
+};
+
+epi_status check_opts(epi_ctx *ctx, const epi_scan_opts *o)
+{
+    if (!o) return set_err(ctx, EPI_E_INVALID, "null options");
+    if (o->test != 'f' && o->test != 'i') return set_err(ctx, EPI_E_INVALID, "test must be 'f' or 'i'");
+    if (o->safe != 0 && o->safe != 1) return set_err(ctx, EPI_E_INVALID, "safe must be 0 or 1");
+    if (o->chunk < 1) return set_err(ctx, EPI_E_INVALID, "chunk must be >= 1");
+    if (o->form < EPI_FORM_AUTO || o->form > EPI_FORM_TENSOR) return set_err(ctx, EPI_E_INVALID, "bad form");
+    if (o->report_trait < -1 || o->report_trait >= ctx->ntraits)
+        return set_err(ctx, EPI_E_INVALID, "report_trait %d out of range", o->report_trait);
+    return EPI_OK;
+}
+
+int pick_form(const epi_ctx *ctx, const epi_scan_opts *o)
+{
+    if (o->form != EPI_FORM_AUTO) return o->form;
+    if (epi::mma_available() && ctx->nid >= epi::mma_min_nid()) return EPI_FORM_TENSOR;
+    return EPI_FORM_POPC;
+}
+
+// Builds the kernel arguments and tile schedule for `blocks` and uploads the schedule.
+epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const epi_scan_opts *o, ScanRun &r)
+{
+    r.form = pick_form(ctx, o);
+    if (r.form == EPI_FORM_TENSOR && !epi::mma_available())
+        return set_err(ctx, EPI_E_UNSUPPORTED, "tensor form not available in this build");
+    if (r.form == EPI_FORM_POPC && ctx->nid > 65535)
+        return set_err(ctx, EPI_E_UNSUPPORTED, "popcount form counts in 16 bits: at most 65535 individuals "
+                       "(the reference's unsigned short counts, EpiOpenCL.c:68)");
+    const int TI = r.form == EPI_FORM_TENSOR ? epi::mma_tile_i() : epi::popc_tile_i();
+    const int TJ = r.form == EPI_FORM_TENSOR ? epi::mma_tile_j() : epi::popc_tile_j();
+    r.desc.resize(nblocks);
+    int64_t base = 0;
+    for (int b = 0; b < nblocks; ++b) {
+        const epi_block &e = blocks[b];
+        if (e.size1 < 0 || e.size2 < 0 || e.start1 < 0 || e.start2 < 0 ||
+            (int64_t)e.start1 + e.size1 > ctx->nsnp || (int64_t)e.start2 + e.size2 > ctx->nsnp)
+            return set_err(ctx, EPI_E_INVALID, "block %d out of range", b);
+        BlockDesc &d = r.desc[b];
+        d.start1 = e.start1;
+        d.size1 = e.size1;
+        d.start2 = e.start2;
+        d.size2 = e.size2;
+        d.tiles_i = (e.size1 + TI - 1) / TI;
+        d.tiles_j = (e.size2 + TJ - 1) / TJ;
+        d.tile_base = base;
+        base += (int64_t)d.tiles_i * d.tiles_j;
+    }
+    r.ntiles = base;
+    size_t bcap = (size_t)ctx->blocks_cap * sizeof(BlockDesc);
+    CK(ensure(&ctx->d_blocks, &bcap, (size_t)std::max(nblocks, 1) * sizeof(BlockDesc)));
+    ctx->blocks_cap = (int)(bcap / sizeof(BlockDesc));
+    if (nblocks)
+        CK(cudaMemcpyAsync(ctx->d_blocks, r.desc.data(), nblocks * sizeof(BlockDesc), cudaMemcpyHostToDevice,
+                           ctx->stream));
+    if (ctx->maxf_cap < 2 * ctx->ntraits) {
+        if (ctx->d_maxf) cudaFree(ctx->d_maxf);
+        ctx->d_maxf = nullptr;
+        CK(cudaMalloc((void **)&ctx->d_maxf, 2 * ctx->ntraits * sizeof(unsigned int)));
+        ctx->maxf_cap = 2 * ctx->ntraits;
+    }
+    epi::ScanArgs &a = r.args;
+    memset(&a, 0, sizeof(a));
+    a.planes = ctx->d_planes;
+    a.codes = ctx->d_codes;
+    a.Wp = ctx->Wp;
+    a.Wc = ctx->Wc;
+    a.nid = ctx->nid;
+    a.y = ctx->d_y;
+    a.q = ctx->d_q;
+    a.wmask = ctx->d_wmask;
+    a.qc = ctx->d_qc;
+    a.Np = ctx->Np;
+    a.ntraits = ctx->ntraits;
+    a.blocks = ctx->d_blocks;
+    a.nblocks = nblocks;
+    a.ntiles = r.ntiles;
+    a.test_int = o->test == 'i';
+    a.safe = o->safe;
+    a.report_trait = o->report_trait;
+    a.t1 = o->t1;
+    a.t2 = o->t2;
+    a.counters = ctx->d_counters;
+    a.maxf = ctx->d_maxf;
+    a.maxf2 = ctx->d_maxf + ctx->ntraits;
+    return EPI_OK;
+}
+
+// Resets the counters and maxima, launches the selected form between the timing events.
+epi_status launch_run(epi_ctx *ctx, ScanRun &r)
+{
+    CK(cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(unsigned long long), ctx->stream));
+    std::vector<unsigned int> init(2 * ctx->ntraits, 0x007fffffu);  // order-encoded -inf
+    CK(cudaMemcpyAsync(ctx->d_maxf, init.data(), init.size() * sizeof(unsigned int), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    ctx->last_launches = 0;
+    if (r.ntiles > 0) {
+        const int grid = (int)std::min<int64_t>(r.ntiles, ctx->sm_count);
+        if (r.form == EPI_FORM_TENSOR) {
+            CK(epi::launch_mma(r.args, grid, ctx->stream));
+        } else {
+            CK(epi::launch_popc(r.args, grid, ctx->stream));
+        }
+        ctx->last_launches = 1;
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    return EPI_OK;
+}
+
+struct HitKey {
+    int32_t trait, block, s, k, l, gx, gy;
+    int64_t idx;
+};
+
+}  // namespace
+
+extern "C" epi_status epi_scan(epi_ctx *ctx, const epi_block *blocks, int32_t nblocks, const epi_scan_opts *opts,
+                               epi_hit *hits, int64_t cap, int64_t *nhits, int32_t *hit_block, int32_t *hit_trait,
+                               float *max_f, float *max_f2)
+{
+    if (!ctx) return EPI_E_INVALID;
+    ctx->err.clear();
+    if (ctx->nid == 0 || ctx->ntraits == 0)
+        return set_err(ctx, EPI_E_STATE, "epi_scan: load genotypes and traits first");
+    if (nblocks < 0 || (nblocks > 0 && !blocks)) return set_err(ctx, EPI_E_INVALID, "epi_scan: bad blocks");
+    if (cap < 0 || (cap > 0 && !hits)) return set_err(ctx, EPI_E_INVALID, "epi_scan: bad hit buffer");
+    epi_status s = check_opts(ctx, opts);
+    if (s != EPI_OK) return s;
+    CK(cudaSetDevice(ctx->device));
+    ScanRun r;
+    s = setup_run(ctx, blocks, nblocks, opts, r);
+    if (s != EPI_OK) return s;
+    if (ctx->hit_cap == 0) {
+        const int64_t initial = 1 << 20;
+        CK(cudaMalloc((void **)&ctx->d_hits, initial * sizeof(DevHit)));
+        ctx->hit_cap = initial;
+    }
+    unsigned long long found = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        r.args.hits = ctx->d_hits;
+        r.args.cap = ctx->hit_cap;
+        s = launch_run(ctx, r);
+        if (s != EPI_OK) return s;
+        CK(cudaMemcpyAsync(&found, ctx->d_counters, sizeof(found), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if ((int64_t)found <= ctx->hit_cap) break;
+        // every hit is needed to put the first `cap` in output order: grow and rescan
+        cudaFree(ctx->d_hits);
+        ctx->d_hits = nullptr;
+        ctx->hit_cap = 0;
+        CK(cudaMalloc((void **)&ctx->d_hits, (size_t)found * sizeof(DevHit)));
+        ctx->hit_cap = (int64_t)found;
+    }
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->last_ms = ms;
+    int64_t pairs = 0;
+    for (int b = 0; b < nblocks; ++b) pairs += block_pairs(blocks[b]);
+    ctx->last_pairs = pairs * ctx->ntraits;
+
+    std::vector<unsigned int> mx(2 * ctx->ntraits);
+    CK(cudaMemcpyAsync(mx.data(), ctx->d_maxf, mx.size() * sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    std::vector<DevHit> dh((size_t)found);
+    if (found)
+        CK(cudaMemcpyAsync(dh.data(), ctx->d_hits, (size_t)found * sizeof(DevHit), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int t = 0; t < ctx->ntraits; ++t) {
+        if (max_f) max_f[t] = epi::ord2f(mx[t]);
+        if (max_f2) max_f2[t] = opts->test == 'i' ? epi::ord2f(mx[ctx->ntraits + t]) : 0.0f;
+    }
+
+    // output order: (trait,) block, result slot, chunk k, chunk l, gx, gy (EpiOpenCL.c:1576-1627)
+    const int L = opts->safe ? 8 : 16;
+    const int chunk = opts->chunk;
+    std::vector<HitKey> keys((size_t)found);
+    for (size_t i = 0; i < keys.size(); ++i) {
+        const DevHit &h = dh[i];
+        const epi_block &b = blocks[h.block];
+        HitKey &k = keys[i];
+        k.trait = opts->report_trait < 0 ? h.trait : 0;
+        k.block = h.block;
+        k.gx = h.snp1 - b.start1;
+        k.gy = h.snp2 - b.start2;
+        k.s = (k.gx % L) * L + (k.gy % L);
+        k.k = k.gx / chunk;
+        k.l = k.gy / chunk;
+        k.idx = (int64_t)i;
+    }
+    std::sort(keys.begin(), keys.end(), [](const HitKey &x, const HitKey &y) {
+        if (x.trait != y.trait) return x.trait < y.trait;
+        if (x.block != y.block) return x.block < y.block;
+        if (x.s != y.s) return x.s < y.s;
+        if (x.k != y.k) return x.k < y.k;
+        if (x.l != y.l) return x.l < y.l;
+        if (x.gx != y.gx) return x.gx < y.gx;
+        return x.gy < y.gy;
+    });
+    const int64_t nout = std::min<int64_t>((int64_t)found, cap);
+    for (int64_t i = 0; i < nout; ++i) {
+        const DevHit &h = dh[(size_t)keys[(size_t)i].idx];
+        hits[i].snp1 = h.snp1;
+        hits[i].snp2 = h.snp2;
+        hits[i].df1 = h.df1;
+        hits[i].df2 = h.df2;
+        hits[i].F = h.F;
+        hits[i].F2 = h.F2;
+        if (hit_block) hit_block[i] = h.block;
+        if (hit_trait) hit_trait[i] = h.trait;
+    }
+    if (nhits) *nhits = (int64_t)found;
+    if ((int64_t)found > cap) return set_err(ctx, EPI_E_OVERFLOW, "%llu hits, capacity %lld", found, (long long)cap);
+    return EPI_OK;
+}
+
+extern "C" epi_status epi_scan_dump(epi_ctx *ctx, const epi_block *block, const epi_scan_opts *opts, int32_t trait,
+                                    int32_t *counts, float *F, float *F2, int32_t *df1, int32_t *df2)
+{
+    if (!ctx) return EPI_E_INVALID;
+    ctx->err.clear();
+    if (ctx->nid == 0 || ctx->ntraits == 0) return set_err(ctx, EPI_E_STATE, "epi_scan_dump: nothing loaded");
+    if (!block) return set_err(ctx, EPI_E_INVALID, "epi_scan_dump: null block");
+    if (trait < 0 || trait >= ctx->ntraits) return set_err(ctx, EPI_E_INVALID, "trait out of range");
+    epi_scan_opts o = *opts;
+    o.report_trait = trait;
+    epi_status s = check_opts(ctx, &o);
+    if (s != EPI_OK) return s;
+    CK(cudaSetDevice(ctx->device));
+    ScanRun r;
+    s = setup_run(ctx, block, 1, &o, r);
+    if (s != EPI_OK) return s;
+    const size_t np = (size_t)block->size1 * block->size2;
+    int32_t *dc = nullptr, *dd1 = nullptr, *dd2 = nullptr;
+    float *dF = nullptr, *dF2 = nullptr;
+    struct Out { void *host; void **dev; size_t bytes; };
+    Out outs[] = {{counts, (void **)&dc, np * 9 * sizeof(int32_t)}, {F, (void **)&dF, np * sizeof(float)},
+                  {F2, (void **)&dF2, np * sizeof(float)}, {df1, (void **)&dd1, np * sizeof(int32_t)},
+                  {df2, (void **)&dd2, np * sizeof(int32_t)}};
+    epi_status st = EPI_OK;
+    for (Out &x : outs) {
+        if (!x.host || !np) continue;
+        cudaError_t e = cudaMalloc(x.dev, x.bytes);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(*x.dev, x.host, x.bytes, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) { st = set_err(ctx, EPI_E_CUDA, "dump buffers: %s", cudaGetErrorString(e)); break; }
+    }
+    if (st == EPI_OK) {
+        r.args.dump_counts = dc;
+        r.args.dump_F = dF;
+        r.args.dump_F2 = dF2;
+        r.args.dump_df1 = dd1;
+        r.args.dump_df2 = dd2;
+        r.args.hits = ctx->d_hits;
+        r.args.cap = 0;
+        st = launch_run(ctx, r);
+    }
+    if (st == EPI_OK) {
+        for (Out &x : outs) {
+            if (!x.host || !*x.dev) continue;
+            cudaError_t e = cudaMemcpyAsync(x.host, *x.dev, x.bytes, cudaMemcpyDeviceToHost, ctx->stream);
+            if (e != cudaSuccess) { st = set_err(ctx, EPI_E_CUDA, "dump readback: %s", cudaGetErrorString(e)); break; }
+        }
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (st == EPI_OK && e != cudaSuccess) st = set_err(ctx, EPI_E_CUDA, "dump: %s", cudaGetErrorString(e));
+    }
+    for (Out &x : outs)
+        if (*x.dev) cudaFree(*x.dev);
+    return st;
+}
+
+extern "C" epi_status epi_last_timing(const epi_ctx *ctx, double *kernel_ms, int64_t *pairs, int32_t *launches)
+{
+    if (!ctx) return EPI_E_INVALID;
+    if (kernel_ms) *kernel_ms = ctx->last_ms;
+    if (pairs) *pairs = ctx->last_pairs;
+    if (launches) *launches = ctx->last_launches;
+    return EPI_OK;
+}

@@ -1,0 +1,59 @@
+// prep.cu -- device-side genotype preparation.
+//
+// Turns the reference's packed rows (src/readplink.c:1066-1102: 16 codes per int32, first
+// individual in bits 31:30, tail word right-aligned with `remain` codes) into
+//   planes  uint4 [nsnp][Wp]: bits of [g==0], [g==1], [g==2], [g!=3] per 32 individuals
+//   codes   uint32 [nsnp][Wc]: 2-bit codes, LSB first, padding individuals coded 3
+// The decoding is the kernel's own (EpiOpenCL.c:116-228), done once per load instead of
+// once per pair.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace epi {
+
+__device__ __forceinline__ uint32_t ref_code(const int32_t *row, int k, int nid, int npack, int remain)
+{
+    if (k >= nid) return 3u;
+    if (k < 16 * npack) return ((uint32_t)row[k >> 4] >> (30 - 2 * (k & 15))) & 3u;
+    const int t = k - 16 * npack;
+    return ((uint32_t)row[npack] >> (2 * (remain - 1 - t))) & 3u;
+}
+
+// One thread per (SNP, 32-individual word).
+__global__ void k_unpack(const int32_t *__restrict__ raw, int nsnp, int nid, int npack, int remain,
+                         int npack1, uint4 *__restrict__ planes, int Wp, uint32_t *__restrict__ codes, int Wc)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)nsnp * Wp;
+    if (gid >= total) return;
+    const int s = (int)(gid / Wp), w = (int)(gid % Wp);
+    const int32_t *row = raw + (size_t)s * npack1;
+    uint32_t p0 = 0, p1 = 0, p2 = 0, c0 = 0, c1 = 0;
+#pragma unroll 4
+    for (int t = 0; t < 32; ++t) {
+        const uint32_t c = ref_code(row, 32 * w + t, nid, npack, remain);
+        p0 |= (uint32_t)(c == 0u) << t;
+        p1 |= (uint32_t)(c == 1u) << t;
+        p2 |= (uint32_t)(c == 2u) << t;
+        if (t < 16) c0 |= c << (2 * t);
+        else c1 |= c << (2 * (t - 16));
+    }
+    planes[(size_t)s * Wp + w] = make_uint4(p0, p1, p2, p0 | p1 | p2);
+    if (codes != nullptr) {
+        if (2 * w < Wc) codes[(size_t)s * Wc + 2 * w] = c0;
+        if (2 * w + 1 < Wc) codes[(size_t)s * Wc + 2 * w + 1] = c1;
+    }
+}
+
+cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int remain, uint4 *planes, int Wp,
+                          uint32_t *codes, int Wc, cudaStream_t stream)
+{
+    const int npack1 = remain ? npack + 1 : npack;
+    const long long total = (long long)nsnp * Wp;
+    const int nt = 256;
+    const long long nb = (total + nt - 1) / nt;
+    k_unpack<<<(unsigned)nb, nt, 0, stream>>>(raw, nsnp, nid, npack, remain, npack1, planes, Wp, codes, Wc);
+    return cudaGetLastError();
+}
+
+}  // namespace epi

@@ -1,0 +1,114 @@
+"""Seeded synthetic inputs of the scan's shape (no public dataset is involved).
+
+Genotypes: per SNP a minor-allele frequency f ~ U(0.05, 0.5) and Hardy-Weinberg codes
+0/1/2 with probabilities (1-f)^2, 2f(1-f), f^2; each call independently missing (code 3)
+with probability `miss`. Packing follows the reference layout (src/readplink.c:1066-1102).
+Phenotypes: N(0,1) (or standardised gamma(2,1)) with a fraction set to -9 (missing), and
+optionally planted interacting pairs whose 3x3 genotype-class effect tables are random,
+mean 0, each explaining `var_frac` of the variance.
+"""
+import numpy as np
+
+
+def genotype_codes(nid, nsnp, seed, maf=(0.05, 0.5), miss=0.01, chunk=4096):
+    """uint8 array (nsnp, nid) of codes 0/1/2/3."""
+    rng = np.random.default_rng(seed)
+    out = np.empty((nsnp, nid), dtype=np.uint8)
+    for s0 in range(0, nsnp, chunk):
+        s1 = min(nsnp, s0 + chunk)
+        f = rng.uniform(maf[0], maf[1], size=(s1 - s0, 1))
+        p0 = (1.0 - f) ** 2
+        p1 = p0 + 2.0 * f * (1.0 - f)
+        u = rng.random((s1 - s0, nid), dtype=np.float32)
+        g = (u >= p0).astype(np.uint8) + (u >= p1).astype(np.uint8)
+        if miss > 0:
+            g[rng.random((s1 - s0, nid), dtype=np.float32) < miss] = 3
+        out[s0:s1] = g
+    return out
+
+
+def pack(codes, chunk=4096):
+    """Reference packing (readplink.c:1066-1102): int32 (nsnp, npack1); 16 codes per word,
+    first individual in bits 31:30; the tail word holds `remain` codes right-aligned."""
+    codes = np.asarray(codes, dtype=np.uint8)
+    nsnp, nid = codes.shape
+    npack, remain = nid // 16, nid % 16
+    npack1 = npack + (1 if remain else 0)
+    out = np.empty((nsnp, npack1), dtype=np.uint32)
+    shifts = (30 - 2 * np.arange(16)).astype(np.uint32)
+    tshifts = (2 * (remain - 1 - np.arange(remain))).astype(np.uint32)
+    for s0 in range(0, nsnp, chunk):
+        s1 = min(nsnp, s0 + chunk)
+        c = codes[s0:s1].astype(np.uint32)
+        if npack:
+            full = c[:, :16 * npack].reshape(s1 - s0, npack, 16) << shifts
+            out[s0:s1, :npack] = np.bitwise_or.reduce(full, axis=2)
+        if remain:
+            out[s0:s1, npack] = np.bitwise_or.reduce(c[:, 16 * npack:] << tshifts, axis=1)
+    return out.view(np.int32)
+
+
+def unpack(gpack, nid):
+    """Inverse of pack (readplink.c:1104-1143)."""
+    w = np.asarray(gpack).view(np.uint32)
+    nsnp = w.shape[0]
+    npack, remain = nid // 16, nid % 16
+    out = np.empty((nsnp, nid), dtype=np.uint8)
+    if npack:
+        shifts = (30 - 2 * np.arange(16)).astype(np.uint32)
+        out[:, :16 * npack] = ((w[:, :npack, None] >> shifts) & 3).reshape(nsnp, 16 * npack)
+    if remain:
+        tshifts = (2 * (remain - 1 - np.arange(remain))).astype(np.uint32)
+        out[:, 16 * npack:] = (w[:, npack, None] >> tshifts) & 3
+    return out
+
+
+def phenotype(nid, seed, miss=0.02, dist="normal"):
+    rng = np.random.default_rng(seed)
+    if dist == "normal":
+        y = rng.standard_normal(nid)
+    elif dist == "gamma":
+        y = rng.gamma(2.0, 1.0, nid)
+        y = (y - 2.0) / np.sqrt(2.0)
+    else:
+        raise ValueError(dist)
+    y = y.astype(np.float32)
+    if miss > 0:
+        y[rng.random(nid) < miss] = -9.0
+    return y
+
+
+def planted_phenotype(codes, pairs, seed, var_frac=0.005, miss=0.01):
+    """N(0,1) noise plus one random mean-0 3x3 genotype-class effect per planted pair
+    (snp_a, snp_b), each scaled to explain `var_frac` of the phenotypic variance."""
+    rng = np.random.default_rng(seed)
+    nid = codes.shape[1]
+    y = rng.standard_normal(nid)
+    for a, b in pairs:
+        ga, gb = codes[a].astype(np.int64), codes[b].astype(np.int64)
+        ok = (ga != 3) & (gb != 3)
+        table = rng.standard_normal((3, 3))
+        eff = np.zeros(nid)
+        eff[ok] = table[ga[ok], gb[ok]]
+        eff[ok] -= eff[ok].mean()
+        sd = eff[ok].std()
+        if sd > 0:
+            eff *= np.sqrt(var_frac) / sd
+        y += eff
+    y = y.astype(np.float32)
+    if miss > 0:
+        y[rng.random(nid) < miss] = -9.0
+    return y
+
+
+def f_threshold(df1, df2, p):
+    """Upper-tail F quantile (scipy): the threshold for a fixed p-value."""
+    from scipy.stats import f
+    return float(f.isf(p, df1, df2))
+
+
+def uneven_block_sizes():
+    """22 chromosome-like blocks, M_c = round(2000 + 22000*((21-c)/21)^1.3705), total 250,000."""
+    sizes = [int(round(2000 + 22000 * ((21 - c) / 21.0) ** 1.3705)) for c in range(22)]
+    sizes[0] += 250000 - sum(sizes)
+    return sizes
