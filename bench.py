@@ -1,0 +1,447 @@
+"""Benchmark of the exhaustive pairwise epistasis scan on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload cfg3] [--form auto|popc|tensor]
+    python bench.py --impl reference ...      the reference's own kernels on the host cores
+
+A step is one full scan of the workload's SNP pairs (test 8 df + 4 df unless the workload
+says otherwise) over synthetic data of the workload's shape. `value` is pairs/s with the
+genotypes and traits already resident in HBM; `e2e` is the same metric through the C ABI
+from host buffers (genotype + trait upload, scan, hit readback inside the timed region).
+Multi-GPU (torchrun): every rank scans its own replica of the workload (weak scaling, no
+collective on the data path); times are device times, max over ranks.
+Prints one JSON line (rank 0).
+"""
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SNP pairs/sec (8df & 4df) on 1 B200: tensor-core vs popcount form, F err<=1e-5"
+
+WORKLOADS = {
+    # name: (nid, chromosome sizes, test, traits, description)
+    "cfg1": (500, [2000], "f", 1, "plain 8 df scan, N=500 individuals, M=2,000 SNPs, 1 chromosome"),
+    "cfg2": (4000, [10000, 10000], "i", 1, "8 df + 4 df scan, N=4,000, M=20,000 SNPs on 2 chromosomes"),
+    "cfg3": (10000, [100000], "i", 1, "8 df + 4 df scan, N=10,000 individuals, M=100,000 SNPs, 1 chromosome"),
+    "cfg4": (5000, [50000], "f", 64, "8 df scan, N=5,000, M=50,000, 64 phenotype columns (permutations)"),
+    "cfg5": (8000, None, "f", 8, "8 df scan, N=8,000, 22 uneven blocks (M=250,000), 8 traits with own masks"),
+}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def gen_packed(nid, nsnp, seed, miss=0.01, chunk=4096):
+    """Seeded genotypes generated on the GPU (HWE, MAF ~ U(0.05, 0.5), `miss` missing calls),
+    packed in the reference layout into pinned host memory."""
+    import torch
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    npack, remain = divmod(nid, 16)
+    npack1 = npack + (1 if remain else 0)
+    out = torch.empty((nsnp, npack1), dtype=torch.int32, pin_memory=True)
+    shifts = torch.tensor([30 - 2 * t for t in range(16)], device=dev, dtype=torch.int64)
+    tsh = torch.tensor([2 * (remain - 1 - t) for t in range(remain)], device=dev, dtype=torch.int64)
+    for s0 in range(0, nsnp, chunk):
+        m = min(chunk, nsnp - s0)
+        f = torch.rand((m, 1), generator=g, device=dev) * 0.45 + 0.05
+        p0 = (1 - f) ** 2
+        p1 = p0 + 2 * f * (1 - f)
+        u = torch.rand((m, nid), generator=g, device=dev)
+        c = (u >= p0).to(torch.int64) + (u >= p1).to(torch.int64)
+        c[torch.rand((m, nid), generator=g, device=dev) < miss] = 3
+        parts = []
+        if npack:
+            parts.append((c[:, :16 * npack].reshape(m, npack, 16) << shifts).sum(-1))
+        if remain:
+            parts.append((c[:, 16 * npack:] << tsh).sum(-1, keepdim=True))
+        w = torch.cat(parts, 1)
+        w = torch.where(w >= 2 ** 31, w - 2 ** 32, w).to(torch.int32)
+        out[s0:s0 + m].copy_(w.cpu())
+    return out.numpy()
+
+
+def workload_data(name, seed=1):
+    from epigpu_b200 import synth
+    nid, sizes, test, ntraits, desc = WORKLOADS[name]
+    if sizes is None:
+        sizes = synth.uneven_block_sizes()
+    nsnp = sum(sizes)
+    gp = gen_packed(nid, nsnp, seed=seed)
+    rng = np.random.default_rng(seed + 7)
+    if ntraits == 1:
+        y = synth.phenotype(nid, seed=seed + 1, miss=0.02 if name == "cfg1" else 0.01)
+        valid = None
+    elif name == "cfg4":
+        from epigpu_b200 import capi
+        base = rng.standard_normal(nid).astype(np.float32)
+        cols = [base] + [capi.permute_phenotype(base, p) for p in range(1, ntraits)]
+        y = np.stack(cols, 1)
+        valid = np.repeat((rng.random(nid) >= 0.01)[:, None], ntraits, 1)
+    else:
+        cols, vcols = [], []
+        for t in range(ntraits):
+            if t % 2 == 0:
+                v = rng.standard_normal(nid)
+            else:
+                v = (rng.gamma(2.0, 1.0, nid) - 2.0) / np.sqrt(2.0)
+            cols.append(v.astype(np.float32))
+            vcols.append(rng.random(nid) >= rng.uniform(0.0, 0.10))
+        y = np.stack(cols, 1)
+        valid = np.stack(vcols, 1)
+    starts = np.cumsum([0] + sizes[:-1])
+    blocks = [(int(starts[i]), sizes[i], int(starts[j]), sizes[j]) for i in range(len(sizes)) for j in range(i + 1)]
+    return dict(nid=nid, nsnp=nsnp, sizes=sizes, test=test, ntraits=ntraits, desc=desc, gpack=gp, y=y,
+                valid=valid, blocks=blocks)
+
+
+def thresholds(nid):
+    from epigpu_b200 import synth
+    return synth.f_threshold(8, nid - 9, 1e-6), synth.f_threshold(4, nid - 9, 1e-6)
+
+
+def block_pairs(b):
+    s1, m1, s2, m2 = b
+    gx = np.arange(m1, dtype=np.int64)
+    return int(np.clip(gx + s1 - s2, 0, m2).sum())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def int8_peak_tops():
+    """cuBLAS int8 GEMM throughput on this GPU (torch._int_mm, 8192^3, best of 10), TOP/s."""
+    import torch
+    n = 8192
+    a = torch.randint(-8, 8, (n, n), dtype=torch.int8, device="cuda")
+    b = torch.randint(-8, 8, (n, n), dtype=torch.int8, device="cuda")
+    for _ in range(3):
+        torch._int_mm(a, b)
+    best = 1e30
+    for _ in range(10):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch._int_mm(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def cpu_baseline(data, test, t1, t2, budget_s=12.0, min_m=200):
+    """The reference's own kernels (oracle A, built from its sources) on the host cores,
+    over a bounded sample: a triangle of the workload's first m SNPs at the workload's N,
+    sized to about `budget_s` seconds."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracles
+    if not oracles.have_ref():
+        return None
+    from epigpu_b200 import capi
+    nid = data["nid"]
+    y = data["y"][:, 0] if data["y"].ndim == 2 else data["y"]
+    threads = os.cpu_count() or 1
+    gp = data["gpack"]
+
+    def run(m):
+        blk = (0, m, 0, m)
+        t = time.perf_counter()
+        _, total = oracles.ref_scan_block(gp[:m], nid, y, blk, test=test, t1=t1, t2=t2, cap=1 << 16,
+                                          nthreads=threads)
+        return time.perf_counter() - t, m * (m - 1) // 2
+
+    dt, pairs = run(min_m)
+    rate = pairs / dt
+    m = int(min(data["nsnp"], max(min_m, (2 * rate * budget_s) ** 0.5)))
+    dt, pairs = run(m)
+    return {"value": pairs / dt, "unit": "pairs/s", "cores": threads, "kind": "reference",
+            "sample": "triangle of the first %d SNPs at N=%d (%d pairs, %s test), %.1f s" % (m, nid, pairs,
+                                                                                         "8df+4df" if test == "i"
+                                                                                         else "8df", dt)}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    name = args.workload
+    nid, sizes, test, ntraits, desc = WORKLOADS[name]
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracles
+    if not oracles.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libepiref.so (the reference's kernels "
+                                                              "built from its sources) is missing"}))
+        return 0
+    from epigpu_b200 import synth
+    nsnp = 4000
+    codes = synth.genotype_codes(nid, nsnp, seed=1)
+    gp = synth.pack(codes)
+    y = synth.phenotype(nid, seed=2, miss=0.01)
+    t1, t2 = thresholds(nid)
+    threads = os.cpu_count() or 1
+    # size the per-step sample to ~8 s on this host
+    probe = 150
+    t = time.perf_counter()
+    oracles.ref_scan_block(gp[:probe], nid, y, (0, probe, 0, probe), test=test, t1=t1, t2=t2, cap=1 << 16,
+                           nthreads=threads)
+    rate = probe * (probe - 1) / 2 / (time.perf_counter() - t)
+    m = int(min(nsnp, max(probe, (2 * rate * 8.0) ** 0.5)))
+    pairs = m * (m - 1) // 2
+    times = []
+    for step in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        oracles.ref_scan_block(gp[:m], nid, y, (0, m, 0, m), test=test, t1=t1, t2=t2, cap=1 << 16,
+                               nthreads=threads)
+        if step >= args.warmup:
+            times.append(time.perf_counter() - t)
+    total = sum(times)
+    value = pairs * len(times) / total
+    sample = ("each step: the reference's OpenCL pair kernels (built as C from its sources) emulating "
+              "perform_scan's launches on %d host threads over a triangle of %d SNPs at N=%d (%d pairs)"
+              % (threads, m, nid, pairs))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": "%s: %s" % (name, desc), "nid": nid, "pairs_per_step": pairs},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
+    ap.add_argument("--form", default="auto", choices=["auto", "popc", "tensor"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--popc-sample", type=int, default=20000,
+                    help="SNPs in the square sample used to time the popcount form next to the tensor form")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    from epigpu_b200 import capi
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+
+    data = workload_data(args.workload, seed=1 + rank)
+    nid, test = data["nid"], data["test"]
+    t1, t2 = thresholds(nid)
+    form = {"auto": capi.FORM_AUTO, "popc": capi.FORM_POPC, "tensor": capi.FORM_TENSOR}[args.form]
+    ctx = capi.Context(local)
+    gname, sms = ctx.device_info()
+    gp, y, valid = data["gpack"], data["y"], data["valid"]
+    ntraits = data["ntraits"]
+    opts = capi.default_opts(test=test, t1=t1, t2=t2, form=form, report_trait=0)
+    blocks = data["blocks"]
+    pairs_step = sum(block_pairs(b) for b in blocks) * ntraits
+
+    def load():
+        ctx.load_packed(gp, nid)
+        if valid is None:
+            ctx.set_phenotype(y)
+        else:
+            ctx.set_traits(y, valid)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    load()
+    # device-resident throughput
+    for _ in range(args.warmup):
+        ctx.scan(blocks, opts, ntraits=ntraits)
+    kernel_ms, launches = [], 0
+    barrier()
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        nhits = 0
+        for _ in range(args.steps):
+            hits, n, ex = ctx.scan(blocks, opts, ntraits=ntraits)
+            ms, _, nl, used = ctx.last_timing()
+            kernel_ms.append(ms)
+            launches += nl
+            nhits = n
+        e1.record(stream)
+        barrier()
+        dev_s = e0.elapsed_time(e1) / 1e3
+    if pg:
+        t = torch.tensor([dev_s], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        dev_s = float(t.item())
+    value = pairs_step * args.steps * world / dev_s
+    used_form = "tensor" if used == capi.FORM_TENSOR else "popc"
+
+    # end to end through the C ABI from host buffers
+    for _ in range(max(1, args.warmup // 2)):
+        load()
+        ctx.scan(blocks, opts, ntraits=ntraits)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        load()
+        hits, n, ex = ctx.scan(blocks, opts, ntraits=ntraits)
+    e1.record(stream)
+    barrier()
+    e2e_s = e0.elapsed_time(e1) / 1e3
+    if pg:
+        t = torch.tensor([e2e_s], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = gp.nbytes + y.nbytes + (valid.nbytes if valid is not None else 0)
+    d2h = n * 32 + 64
+
+    # popcount form on a square sample, when the headline form is the tensor form
+    popc = None
+    if used_form == "tensor" and args.popc_sample > 0:
+        m = min(args.popc_sample, data["sizes"][0])
+        popc_blocks = [(0, m, 0, m)]
+        po = capi.default_opts(test=test, t1=t1, t2=t2, form=capi.FORM_POPC)
+        ctx.scan(popc_blocks, po, ntraits=ntraits)
+        ctx.scan(popc_blocks, po, ntraits=ntraits)
+        ms, pp, _, _ = ctx.last_timing()
+        popc = {"value": pp / (ms / 1e3), "unit": "pairs/s", "sample": "%d-SNP triangle" % m}
+
+    out = None
+    if rank == 0:
+        peaks, peak_kind = measured_peaks()
+        clocks = clk.summary()
+        kern_s = statistics.mean(kernel_ms) / 1e3
+        pairs_launch = pairs_step
+        if used_form == "tensor":
+            int8 = int8_peak_tops()
+            ops_pair = 2.0 * 38.4 * nid  # int8 ops per pair (MMA shape 128x192 per 40x16 pairs)
+            achieved = pairs_launch * ops_pair / kern_s / 1e12
+            roof = {"bound": "tensor", "achieved": achieved, "peak": int8, "unit": "TOP/s",
+                    "frac": achieved / int8, "traffic": None,
+                    "peak_source": "cuBLAS int8 GEMM measured in this run (torch._int_mm 8192^3)"}
+        else:
+            # plain form: 10 FP32 FMAs per pair and individual (9 cell sums + sum of squares)
+            # against the FP32 FMA issue peak at the sampled SM clock
+            mhz = clocks["sm_mhz"] or 1965.0
+            peak = sms * 128 * mhz * 1e6 / 1e12
+            achieved = pairs_launch * 10.0 * nid / kern_s / 1e12
+            roof = {"bound": "alu", "achieved": achieved, "peak": peak, "unit": "TFMA/s",
+                    "frac": achieved / peak, "traffic": None,
+                    "peak_source": "%d SMs x 128 FP32 lanes x %.0f MHz sampled SM clock" % (sms, mhz)}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(data, test, t1, t2)
+        out = {
+            "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int8" if used_form == "tensor" else "fp32",
+            "data": "synthetic",
+            "config": {"workload": "%s: %s" % (args.workload, data["desc"]), "nid": nid, "nsnp": data["nsnp"],
+                       "blocks": len(blocks), "traits": ntraits, "test": test, "t1": t1, "t2": t2,
+                       "pairs_per_step": pairs_step, "form": used_form, "hits_per_step": int(nhits),
+                       "l2": "inputs larger than L2 (packed genotypes %.0f MB)" % (gp.nbytes / 1e6),
+                       "gpu": gname},
+            "e2e": {"value": pairs_step * args.steps * world / e2e_s, "unit": "pairs/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "kernel_ms_per_step": statistics.mean(kernel_ms),
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        if popc:
+            out["popc_form"] = popc
+            out["tensor_over_popc"] = value / world / popc["value"]
+        print(json.dumps(out))
+    ctx.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -27,7 +27,7 @@ FORM_AUTO, FORM_POPC, FORM_TENSOR = 0, 1, 2
 EXPORTS = (
     "epi_default_opts", "epi_open", "epi_close", "epi_strerror", "epi_last_error",
     "epi_device_info", "epi_load_packed", "epi_set_traits", "epi_set_phenotype", "epi_scan",
-    "epi_scan_dump", "epi_last_timing", "epi_permute_phenotype",
+    "epi_scan_dump", "epi_last_timing", "epi_get_stream", "epi_permute_phenotype",
 )
 
 
@@ -67,7 +67,8 @@ _SIGS = {
     "epi_scan_dump": (ctypes.c_int, [_P, ctypes.POINTER(Block), ctypes.POINTER(ScanOpts), ctypes.c_int32,
                                      _P, _P, _P, _P, _P]),
     "epi_last_timing": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64),
-                                       ctypes.POINTER(ctypes.c_int32)]),
+                                       ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
+    "epi_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     "epi_permute_phenotype": (None, [_P, ctypes.c_int32, ctypes.c_uint32]),
 }
 
@@ -221,13 +222,21 @@ class Context:
                         "epi_scan_dump")
         return {"counts": counts, "F": F, "F2": F2, "df1": d1, "df2": d2}
 
+    def stream_handle(self):
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        h = ctypes.c_void_p()
+        self._check(self.lib.epi_get_stream(self.h, ctypes.byref(h)), "epi_get_stream")
+        return h.value or 0
+
     def last_timing(self):
+        """(kernel ms, pair tests, kernel launches, form) of the last scan."""
         ms = ctypes.c_double()
         pairs = ctypes.c_int64()
         nl = ctypes.c_int32()
-        self._check(self.lib.epi_last_timing(self.h, ctypes.byref(ms), ctypes.byref(pairs), ctypes.byref(nl)),
-                    "epi_last_timing")
-        return ms.value, pairs.value, nl.value
+        form = ctypes.c_int32()
+        self._check(self.lib.epi_last_timing(self.h, ctypes.byref(ms), ctypes.byref(pairs), ctypes.byref(nl),
+                                             ctypes.byref(form)), "epi_last_timing")
+        return ms.value, pairs.value, nl.value, form.value
 
 
 def permute_phenotype(phen, seed):

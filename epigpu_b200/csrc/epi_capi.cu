@@ -69,6 +69,7 @@ struct epi_ctx {
     double last_ms = 0.0;
     int64_t last_pairs = 0;
     int last_launches = 0;
+    int last_form = 0;
     std::string err;
 };
 
@@ -426,6 +427,7 @@ epi_status launch_run(epi_ctx *ctx, ScanRun &r)
                        ctx->stream));
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     ctx->last_launches = 0;
+    ctx->last_form = r.form;
     if (r.ntiles > 0) {
         const int grid = (int)std::min<int64_t>(r.ntiles, ctx->sm_count);
         if (r.form == EPI_FORM_TENSOR) {
@@ -600,9 +602,18 @@ extern "C" epi_status epi_scan_dump(epi_ctx *ctx, const epi_block *block, const 
     return st;
 }
 
-extern "C" epi_status epi_last_timing(const epi_ctx *ctx, double *kernel_ms, int64_t *pairs, int32_t *launches)
+extern "C" epi_status epi_get_stream(const epi_ctx *ctx, void **stream)
+{
+    if (!ctx || !stream) return EPI_E_INVALID;
+    *stream = (void *)ctx->stream;
+    return EPI_OK;
+}
+
+extern "C" epi_status epi_last_timing(const epi_ctx *ctx, double *kernel_ms, int64_t *pairs, int32_t *launches,
+                                      int32_t *form)
 {
     if (!ctx) return EPI_E_INVALID;
+    if (form) *form = ctx->last_form;
     if (kernel_ms) *kernel_ms = ctx->last_ms;
     if (pairs) *pairs = ctx->last_pairs;
     if (launches) *launches = ctx->last_launches;

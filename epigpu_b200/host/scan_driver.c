@@ -1,0 +1,278 @@
+/*
+ * scan_driver.c -- perform_scan on the B200: the drop-in for src/EpiOpenCL.c:1312-1686.
+ *
+ * Same signature, same globals, same results file:
+ *   header (EpiOpenCL.c:1459-1470), then per chromosome block (i, j <= i) in order a line
+ *   "# i x j : n interactions" (:1618) and n rows (:1632-1653):
+ *     SNP1 (1-based) SNP1name Chr1 SNP2 SNP2name Chr2 df1 df2 F [F2]
+ * and the same checkpoint/resume rule: an existing results file is validated against the
+ * data and the scan restarts after its last complete block (resume, :1187-1274).
+ * The OpenCL set-up, buffers and chunk launches are replaced by libepigpu.so: all the
+ * remaining blocks go to the GPU in batches, each batch in one persistent launch; every
+ * block's section is appended as soon as its batch returns.
+ *
+ * Differences from the reference, on purpose:
+ *  - a resumed scan restarts at column s2 only in row s1; the reference starts every later
+ *    row at s2 as well (EpiOpenCL.c:1540) and so skips blocks (i > s1, j < s2);
+ *  - hits are counted with atomics and returned in the reference's serial order instead
+ *    of 200-row slots written without synchronisation (EpiOpenCL.c:253-255), so no hit is
+ *    lost or overwritten whatever the count;
+ *  - errors print the library's message and exit with its status (ereport, :1159-1177).
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "epigpu_host.h"
+
+#define PAIR_BATCH ((long long)1 << 34) /* pairs per launch batch between checkpoints */
+
+static void fail(epi_ctx *ctx, epi_status st, const char *what)
+{
+    if (st == EPI_E_NODEVICE) {
+        printf("\n\nError:\nThere is no suitable GPU on this computer.\nThis build requires an NVIDIA B200 "
+               "(sm_100a) device; -d selects it.\n\n");
+        exit(1);
+    }
+    printf("\n\nThere was an error.\n%s: %s\n%s\n", what, epi_strerror(st), ctx ? epi_last_error(ctx) : "");
+    exit((int)st);
+}
+
+/* src/EpiOpenCL.c:1187-1274. Returns 0 = fresh start, 1 = resume, exits on mismatch. */
+int resume_point(const char *filename, int *chr1, int *chr2, int *tothits, int nid, int nsnp)
+{
+    char line[512], name[300];
+    int v = 0, c1 = 0, c2 = 0, k = 0, blocks = 0;
+    float th1 = 0, th2 = 0;
+    char x = 0;
+    *chr1 = *chr2 = 0;
+    FILE *in = fopen(filename, "rt");
+    if (!in) return 0;
+    name[0] = 0;
+    if (!fgets(line, sizeof(line), in) || sscanf(line, "Datafile: %299s", name) != 1 || strcmp(name, plinkbin) != 0) {
+        printf("Can't resume analysis with different datafile!\n");
+        exit(1);
+    }
+    if (!fgets(line, sizeof(line), in) || sscanf(line, "Number of individuals: %d", &v) != 1 || v != nid) {
+        printf("Can't resume analysis with different data!\n");
+        exit(1);
+    }
+    if (!fgets(line, sizeof(line), in) || sscanf(line, "Number of SNPs: %d", &v) != 1 || v != nsnp) {
+        printf("Can't resume analysis with different data!\n");
+        exit(1);
+    }
+    if (!fgets(line, sizeof(line), in) || sscanf(line, "Permutation: %d", &v) != 1 || v != UPERM) {
+        printf("Can't resume analysis with different permutation!\n");
+        exit(1);
+    }
+    if (fgets(line, sizeof(line), in) && sscanf(line, "Threshold: %f %f", &th1, &th2) == 2) {
+        if (th1 != UTHRESHOLD1)
+            printf("Warning: Resuming analysis with different full threshold, changed from %f to %f\n", th1,
+                   UTHRESHOLD1);
+        if (th2 != UTHRESHOLD2)
+            printf("Warning: Resuming analysis with different interaction threshold, changed from %f to %f\n", th2,
+                   UTHRESHOLD2);
+    }
+    if (!fgets(line, sizeof(line), in) || sscanf(line, "Test: %c", &x) != 1 || x != UTEST) {
+        printf("Can't resume analysis performing a different test!\n");
+        exit(1);
+    }
+    if (!fgets(line, sizeof(line), in) || !fgets(line, sizeof(line), in)) { /* blank line, column names */
+        fclose(in);
+        return 1;
+    }
+    /* count complete blocks: a block header followed by all of its rows */
+    while (fgets(line, sizeof(line), in)) {
+        int a, b, n;
+        if (sscanf(line, "# %d x %d : %d interactions", &a, &b, &n) != 3) break;
+        int rows = 0;
+        while (rows < n && fgets(line, sizeof(line), in)) ++rows;
+        if (rows < n) break; /* a block cut short is rescanned */
+        c1 = a;
+        c2 = b;
+        k = n;
+        *tothits += k;
+        ++blocks;
+    }
+    fclose(in);
+    if (blocks) {
+        if (c1 == c2) {
+            *chr1 = c1 + 1;
+            *chr2 = 0;
+        } else {
+            *chr1 = c1;
+            *chr2 = c2 + 1;
+        }
+    }
+    return 1;
+}
+
+/* EpiOpenCL.c:1459-1470 */
+static void write_header_full(const char *filename, int nid, int nsnp)
+{
+    FILE *out = fopen(filename, "wt");
+    if (!out) {
+        printf("Cannot write %s\n", filename);
+        exit(1);
+    }
+    fprintf(out, "Datafile: %s %s\n", plinkbin, UPHEN);
+    fprintf(out, "Number of individuals: %d\nNumber of SNPs: %d\nPermutation: %d\nThreshold: %f %f\n", nid, nsnp,
+            UPERM, UTHRESHOLD1, UTHRESHOLD2);
+    if (UTEST == 'f') {
+        fprintf(out, "Test: full\n\n");
+        fprintf(out, "SNP1\tSNP1name\tChr1\tSNP2\tSNP2name\tChr2\tdf1\tdf2\tFval\n");
+    } else {
+        fprintf(out, "Test: interactions + full\n\n");
+        fprintf(out, "SNP1\tSNP1name\tChr1\tSNP2\tSNP2name\tChr2\tdf1\tdf2\tFval\tFint\n");
+    }
+    fclose(out);
+}
+
+int perform_scan(int *geno, chromosome *chrstat, ped *dat, map *genmap, int nid, int nsnp, int npack, int remain,
+                 int nchr, char *filename)
+{
+    const double t_start = wall_seconds();
+    epi_ctx *ctx = NULL;
+    epi_status st = epi_open(UDEVICE, &ctx);
+    if (st != EPI_OK) fail(NULL, st, "opening the GPU");
+    {
+        char name[256];
+        int sms = 0;
+        epi_device_info(ctx, name, sizeof(name), &sms);
+        printf("\nUsing device %d: %s (%d SMs)\n\n", UDEVICE, name, sms);
+    }
+
+    int s1 = 0, s2 = 0, tothits = 0;
+    const int chrint = nchr * (nchr + 1) / 2;
+    int ccount = 0;
+    if (resume_point(filename, &s1, &s2, &tothits, nid, nsnp) && (s1 != 0 || s2 != 0)) {
+        ccount = s1 * (s1 + 1) / 2 + s2;
+        if (ccount == chrint) {
+            printf("Scan already completed!\n\n");
+            epi_close(ctx);
+            return tothits;
+        } else if (ccount > chrint) {
+            printf("The initial analysis was performed with a different dataset!\nPlease use a different "
+                   "filename.\n");
+            exit(1);
+        }
+        printf("Resuming from %d/%d, %d hits found so far...\n\n", ccount + 1, chrint, tothits);
+    } else {
+        write_header_full(filename, nid, nsnp);
+    }
+
+    st = epi_load_packed(ctx, (const int32_t *)geno, nid, nsnp, npack, remain);
+    if (st != EPI_OK) fail(ctx, st, "loading genotypes");
+    float *phen = (float *)malloc(sizeof(float) * (size_t)nid);
+    for (int i = 0; i < nid; i++) phen[i] = dat[i].phen;
+    st = epi_set_phenotype(ctx, phen, nid, USAFE);
+    if (st != EPI_OK) fail(ctx, st, "loading the phenotype");
+    free(phen);
+
+    epi_scan_opts opts;
+    epi_default_opts(&opts);
+    opts.test = UTEST;
+    opts.safe = USAFE;
+    opts.chunk = UCHUNKSIZE;
+    opts.t1 = UTHRESHOLD1;
+    opts.t2 = UTHRESHOLD2;
+    opts.form = UFORM;
+    opts.report_trait = 0;
+
+    /* remaining blocks in perform_scan's order */
+    epi_block *blocks = (epi_block *)malloc(sizeof(epi_block) * (size_t)(chrint > 0 ? chrint : 1));
+    int *bi = (int *)malloc(sizeof(int) * (size_t)(chrint > 0 ? chrint : 1));
+    int *bj = (int *)malloc(sizeof(int) * (size_t)(chrint > 0 ? chrint : 1));
+    int nb = 0;
+    for (int i = s1; i < nchr; i++) {
+        for (int j = (i == s1 ? s2 : 0); j <= i; j++) {
+            blocks[nb].start1 = chrstat[i].chrstart;
+            blocks[nb].size1 = chrstat[i].chrsize;
+            blocks[nb].start2 = chrstat[j].chrstart;
+            blocks[nb].size2 = chrstat[j].chrsize;
+            bi[nb] = i;
+            bj[nb] = j;
+            ++nb;
+        }
+    }
+
+    int64_t cap = 1 << 20;
+    epi_hit *hits = (epi_hit *)malloc(sizeof(epi_hit) * (size_t)cap);
+    int32_t *hblock = (int32_t *)malloc(sizeof(int32_t) * (size_t)cap);
+    double gpu_ms = 0.0;
+    int b0 = 0;
+    while (b0 < nb) {
+        /* batch of whole blocks up to PAIR_BATCH pairs */
+        long long pairs = 0;
+        int b1 = b0;
+        while (b1 < nb && (b1 == b0 || pairs + (long long)blocks[b1].size1 * blocks[b1].size2 <= PAIR_BATCH)) {
+            pairs += (long long)blocks[b1].size1 * blocks[b1].size2;
+            ++b1;
+        }
+        for (int b = b0; b < b1; ++b)
+            printf("%d/%d\tScanning %s vs %s\n", ++ccount, chrint, chrstat[bi[b]].chrname, chrstat[bj[b]].chrname);
+        fflush(stdout);
+        int64_t n = 0;
+        st = epi_scan(ctx, blocks + b0, b1 - b0, &opts, hits, cap, &n, hblock, NULL, NULL, NULL);
+        if (st == EPI_E_OVERFLOW) {
+            free(hits);
+            free(hblock);
+            cap = n;
+            hits = (epi_hit *)malloc(sizeof(epi_hit) * (size_t)cap);
+            hblock = (int32_t *)malloc(sizeof(int32_t) * (size_t)cap);
+            if (!hits || !hblock) {
+                printf("Out of host memory for %lld results\n", (long long)n);
+                exit(1);
+            }
+            st = epi_scan(ctx, blocks + b0, b1 - b0, &opts, hits, cap, &n, hblock, NULL, NULL, NULL);
+        }
+        if (st != EPI_OK) fail(ctx, st, "scanning");
+        double ms = 0.0;
+        epi_last_timing(ctx, &ms, NULL, NULL, NULL);
+        gpu_ms += ms;
+
+        FILE *out = fopen(filename, "a");
+        if (!out) {
+            printf("Cannot append to %s\n", filename);
+            exit(1);
+        }
+        int64_t h = 0;
+        for (int b = b0; b < b1; ++b) {
+            const int i = bi[b], j = bj[b];
+            int64_t h_end = h;
+            while (h_end < n && hblock[h_end] == b - b0) ++h_end;
+            const int tn = (int)(h_end - h);
+            printf("\n\t%d interactions found in %s vs %s\n", tn, chrstat[i].chrname, chrstat[j].chrname);
+            fprintf(out, "# %d x %d : %d interactions\n", i, j, tn);
+            for (; h < h_end; ++h) {
+                const epi_hit *r = &hits[h];
+                if (UTEST == 'f')
+                    fprintf(out, "%d\t%s\t%s\t%d\t%s\t%s\t%d\t%d\t%f\n", r->snp1 + 1, genmap[r->snp1].snpname,
+                            chrstat[i].chrname, r->snp2 + 1, genmap[r->snp2].snpname, chrstat[j].chrname, r->df1,
+                            r->df2, r->F);
+                else
+                    fprintf(out, "%d\t%s\t%s\t%d\t%s\t%s\t%d\t%d\t%f\t%f\n", r->snp1 + 1, genmap[r->snp1].snpname,
+                            chrstat[i].chrname, r->snp2 + 1, genmap[r->snp2].snpname, chrstat[j].chrname, r->df1,
+                            r->df2, r->F, r->F2);
+                ++tothits;
+            }
+        }
+        fclose(out);
+        char tt[64];
+        format_duration(tt, sizeof(tt), ms / 1000.0);
+        printf("\n\t%d blocks scanned on the GPU in %s (%.3f s)\n\n", b1 - b0, tt, ms / 1000.0);
+        b0 = b1;
+    }
+    free(hits);
+    free(hblock);
+    free(blocks);
+    free(bi);
+    free(bj);
+    epi_close(ctx);
+
+    char tt[64];
+    format_duration(tt, sizeof(tt), wall_seconds() - t_start);
+    printf("\nProgramme finished in %s (GPU %.3f s)\n%d epistatic interactions discovered\n", tt, gpu_ms / 1000.0,
+           tothits);
+    return tothits;
+}

@@ -5,7 +5,7 @@
  * It replaces the device side of epiGPU's scan: the OpenCL pair kernels of
  * src/EpiOpenCL.c:45-963 and the platform/buffer/launch/readback code of perform_scan
  * (src/EpiOpenCL.c:1383-1436, :1473-1627). The host program keeps epiGPU's CLI, its
- * .epigpu input and its results file (epigpu_b200/host/*.c). Only plain C types cross
+ * .epigpu input and its results file (the C host program in epigpu_b200/host). Only plain C types cross
  * this boundary: host pointers and sizes, no CUDA or torch types.
  *
  * Conventions
@@ -138,9 +138,15 @@ epi_status epi_scan_dump(epi_ctx *ctx, const epi_block *block, const epi_scan_op
                          int32_t *df1, int32_t *df2);
 
 /* Device time of the last epi_scan's pair kernels (CUDA events on the scan stream),
- * the pairs they tested, and how many kernels were launched. */
+ * the pair tests they made (pairs x traits), how many kernels were launched and which
+ * form ran (EPI_FORM_POPC or EPI_FORM_TENSOR). Any output may be NULL. */
 epi_status epi_last_timing(const epi_ctx *ctx, double *kernel_ms, int64_t *pairs,
-                           int32_t *launches);
+                           int32_t *launches, int32_t *form);
+
+/* The context's CUDA stream (a cudaStream_t, returned as an opaque pointer): every copy
+ * and kernel of the context runs on it, so a caller can order or time its own work
+ * against the scan. */
+epi_status epi_get_stream(const epi_ctx *ctx, void **stream);
 
 /* The permutation of src/main.c:336-348 applied to a phenotype vector: srand(seed), then
  * glibc rand() Fisher-Yates from the end. Matches `epiGPU -A ... -p seed`. */
