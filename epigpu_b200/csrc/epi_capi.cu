@@ -20,7 +20,10 @@
 
 namespace epi {
 cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int remain, uint4 *planes, int Wp,
-                          uint32_t *codes, int Wc, cudaStream_t stream);
+                          uint32_t *codes, int Wc, uint8_t *hcodes, uint32_t *missbits, uint32_t *misssum, int Ws,
+                          cudaStream_t stream);
+cudaError_t launch_qmiss(const uint32_t *missbits, int nsnp, int Wp, const uint32_t *wmask, const double *qd, int Np,
+                         int ntraits, double *qm, cudaStream_t stream);
 cudaError_t launch_popc(const ScanArgs &a, int grid, cudaStream_t stream);
 int popc_tile_i();
 int popc_tile_j();
@@ -29,7 +32,9 @@ bool mma_available();
 int mma_tile_i();
 int mma_tile_j();
 int mma_min_nid();
-cudaError_t launch_mma(const ScanArgs &a, int grid, cudaStream_t stream);
+cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream);
+cudaError_t mma_encode_genotypes(MmaMaps *maps, const uint8_t *hcodes, int nsnp, int Np);
+cudaError_t mma_encode_traits(MmaMaps *maps, const int8_t *ydig, int ntraits, int Np);
 }  // namespace epi
 
 using epi::BlockDesc;
@@ -43,19 +48,22 @@ struct epi_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // genotypes
     int nid = 0, nsnp = 0, npack = 0, remain = 0;
-    int Wp = 0, Wc = 0, Np = 0;
+    int Wp = 0, Wc = 0, Ws = 0, Np = 0;
     int32_t *d_raw = nullptr;
     size_t raw_cap = 0;
     uint4 *d_planes = nullptr;
-    uint32_t *d_codes = nullptr;
-    size_t planes_cap = 0, codes_cap = 0;
+    uint8_t *d_hcodes = nullptr;
+    uint32_t *d_missbits = nullptr, *d_misssum = nullptr;
+    size_t planes_cap = 0, hcodes_cap = 0, missbits_cap = 0, misssum_cap = 0;
     // traits
     int ntraits = 0, traits_nid = 0;
     float *d_y = nullptr, *d_q = nullptr;
     uint32_t *d_wmask = nullptr;
-    double *d_qc = nullptr, *d_yscale = nullptr, *d_qscale = nullptr;
+    double *d_qc = nullptr, *d_yscale = nullptr, *d_qd = nullptr, *d_qtot = nullptr, *d_qm = nullptr;
     int8_t *d_ydig = nullptr;
-    size_t traits_cap = 0, ydig_cap = 0;
+    size_t traits_cap = 0, ydig_cap = 0, qd_cap = 0, qm_cap = 0;
+    bool qm_valid = false;
+    epi::MmaMaps maps;
     std::vector<double> qc;
     // scan scratch
     DevHit *d_hits = nullptr;
@@ -171,9 +179,9 @@ epi_status epi_close(epi_ctx *ctx)
     if (!ctx) return EPI_OK;
     if (ctx->device >= 0) cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    void *bufs[] = {ctx->d_raw, ctx->d_planes, ctx->d_codes, ctx->d_y, ctx->d_q, ctx->d_wmask, ctx->d_qc,
-                    ctx->d_yscale, ctx->d_qscale, ctx->d_ydig, ctx->d_hits, ctx->d_counters, ctx->d_maxf,
-                    ctx->d_blocks};
+    void *bufs[] = {ctx->d_raw, ctx->d_planes, ctx->d_hcodes, ctx->d_missbits, ctx->d_misssum, ctx->d_y, ctx->d_q,
+                    ctx->d_wmask, ctx->d_qc, ctx->d_yscale, ctx->d_qd, ctx->d_qtot, ctx->d_qm, ctx->d_ydig,
+                    ctx->d_hits, ctx->d_counters, ctx->d_maxf, ctx->d_blocks};
     for (void *p : bufs)
         if (p) cudaFree(p);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -204,13 +212,20 @@ epi_status epi_load_packed(epi_ctx *ctx, const int32_t *gpack, int32_t nid, int3
     const int npack1 = remain ? npack + 1 : npack;
     const int Wp = ((nid + 31) / 32 + 3) / 4 * 4;  // multiple of 4 words = 128 individuals
     const int Wc = 2 * Wp;
+    const int Ws = (Wp + 31) / 32;
     CK(ensure(&ctx->d_raw, &ctx->raw_cap, (size_t)nsnp * npack1 * sizeof(int32_t)));
     CK(ensure(&ctx->d_planes, &ctx->planes_cap, (size_t)nsnp * Wp * sizeof(uint4)));
-    CK(ensure(&ctx->d_codes, &ctx->codes_cap, (size_t)nsnp * Wc * sizeof(uint32_t)));
+    CK(ensure(&ctx->d_hcodes, &ctx->hcodes_cap, (size_t)nsnp * Wp * 32));
+    CK(ensure(&ctx->d_missbits, &ctx->missbits_cap, (size_t)nsnp * Wp * sizeof(uint32_t)));
+    CK(ensure(&ctx->d_misssum, &ctx->misssum_cap, (size_t)nsnp * Ws * sizeof(uint32_t)));
     CK(cudaMemcpyAsync(ctx->d_raw, gpack, (size_t)nsnp * npack1 * sizeof(int32_t), cudaMemcpyHostToDevice,
                        ctx->stream));
-    CK(epi::launch_unpack(ctx->d_raw, nsnp, nid, npack, remain, ctx->d_planes, Wp, ctx->d_codes, Wc, ctx->stream));
+    CK(epi::launch_unpack(ctx->d_raw, nsnp, nid, npack, remain, ctx->d_planes, Wp, nullptr, Wc, ctx->d_hcodes,
+                          ctx->d_missbits, ctx->d_misssum, Ws, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    ctx->Ws = Ws;
+    ctx->qm_valid = false;
+    CK(epi::mma_encode_genotypes(&ctx->maps, ctx->d_hcodes, nsnp, 32 * Wp));
     if (ctx->traits_nid != nid) ctx->ntraits = 0;  // traits no longer match
     ctx->nid = nid;
     ctx->nsnp = nsnp;
@@ -265,6 +280,42 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
             }
         }
     }
+    // tensor form: balanced base-256 digits of round(y * 2^sy) (|Y| <= 8355711 fits three
+    // int8 digits), the valid flag, and the quantised y^2
+    std::vector<int8_t> hd((size_t)ntraits * 4 * Np, 0);
+    std::vector<double> hqd((size_t)ntraits * Np, 0.0), hqtot(ntraits, 0.0), hsc(ntraits, 1.0);
+    for (int t = 0; t < ntraits; ++t) {
+        const float *yt = y + (size_t)t * nid;
+        double sum = 0.0;
+        long long nv = 0;
+        for (int k = 0; k < nid; ++k)
+            if (hw[(size_t)t * Wp + k / 32] >> (k % 32) & 1u) {
+                sum += (double)yt[k];
+                ++nv;
+            }
+        const double mu = nv ? sum / (double)nv : 0.0;
+        double maxabs = 0.0;
+        for (int k = 0; k < nid; ++k)
+            if (hw[(size_t)t * Wp + k / 32] >> (k % 32) & 1u) maxabs = std::max(maxabs, std::fabs((double)yt[k] - mu));
+        const int sy = (maxabs > 0.0 && std::isfinite(maxabs)) ? (int)std::floor(std::log2(8355000.0 / maxabs)) : 0;
+        const double scale = std::ldexp(1.0, sy);
+        hsc[t] = std::ldexp(1.0, -sy);
+        int8_t *d0 = hd.data() + (size_t)t * 4 * Np;
+        for (int k = 0; k < nid; ++k) {
+            if (!(hw[(size_t)t * Wp + k / 32] >> (k % 32) & 1u)) continue;
+            long long Y = std::llround(((double)yt[k] - mu) * scale);
+            Y = std::min(8355711LL, std::max(-8355711LL, Y));
+            const long long a0 = ((Y + 128) & 255) - 128, Y1 = (Y - a0) / 256;
+            const long long a1 = ((Y1 + 128) & 255) - 128, a2 = (Y1 - a1) / 256;
+            d0[k] = 1;
+            d0[Np + k] = (int8_t)a0;
+            d0[2 * (size_t)Np + k] = (int8_t)a1;
+            d0[3 * (size_t)Np + k] = (int8_t)a2;
+            const double yq = (double)Y * hsc[t];
+            hqd[(size_t)t * Np + k] = yq * yq;
+            hqtot[t] += yq * yq;
+        }
+    }
     size_t need = (size_t)ntraits * Np * sizeof(float);
     size_t cap_y = ctx->traits_cap, cap_q = ctx->traits_cap;
     CK(ensure(&ctx->d_y, &cap_y, need));
@@ -281,9 +332,24 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
     CK(cudaMemcpyAsync(ctx->d_q, hq.data(), need, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->d_wmask, hw.data(), hw.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->d_qc, ctx->qc.data(), ntraits * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(ensure(&ctx->d_ydig, &ctx->ydig_cap, hd.size()));
+    CK(ensure(&ctx->d_qd, &ctx->qd_cap, hqd.size() * sizeof(double)));
+    if (ctx->d_qtot) cudaFree(ctx->d_qtot);
+    if (ctx->d_yscale) cudaFree(ctx->d_yscale);
+    ctx->d_qtot = nullptr;
+    ctx->d_yscale = nullptr;
+    size_t c1 = 0, c2 = 0;
+    CK(ensure(&ctx->d_qtot, &c1, (size_t)ntraits * sizeof(double)));
+    CK(ensure(&ctx->d_yscale, &c2, (size_t)ntraits * sizeof(double)));
+    CK(cudaMemcpyAsync(ctx->d_ydig, hd.data(), hd.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(epi::mma_encode_traits(&ctx->maps, ctx->d_ydig, ntraits, Np));
+    CK(cudaMemcpyAsync(ctx->d_qd, hqd.data(), hqd.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_qtot, hqtot.data(), ntraits * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_yscale, hsc.data(), ntraits * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->ntraits = ntraits;
     ctx->traits_nid = nid;
+    ctx->qm_valid = false;
     return EPI_OK;
 }
 
@@ -391,13 +457,28 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
         CK(cudaMalloc((void **)&ctx->d_maxf, 2 * ctx->ntraits * sizeof(unsigned int)));
         ctx->maxf_cap = 2 * ctx->ntraits;
     }
+    if (r.form == EPI_FORM_TENSOR && !ctx->qm_valid) {
+        CK(ensure(&ctx->d_qm, &ctx->qm_cap, (size_t)ctx->ntraits * ctx->nsnp * sizeof(double)));
+        CK(epi::launch_qmiss(ctx->d_missbits, ctx->nsnp, ctx->Wp, ctx->d_wmask, ctx->d_qd, ctx->Np, ctx->ntraits,
+                             ctx->d_qm, ctx->stream));
+        ctx->qm_valid = true;
+    }
     epi::ScanArgs &a = r.args;
     memset(&a, 0, sizeof(a));
     a.planes = ctx->d_planes;
-    a.codes = ctx->d_codes;
+    a.hcodes = ctx->d_hcodes;
+    a.missbits = ctx->d_missbits;
+    a.misssum = ctx->d_misssum;
     a.Wp = ctx->Wp;
     a.Wc = ctx->Wc;
+    a.Ws = ctx->Ws;
     a.nid = ctx->nid;
+    a.nsnp = ctx->nsnp;
+    a.yscale = ctx->d_yscale;
+    a.qd = ctx->d_qd;
+    a.qtot = ctx->d_qtot;
+    a.qm = ctx->d_qm;
+    a.ydig = ctx->d_ydig;
     a.y = ctx->d_y;
     a.q = ctx->d_q;
     a.wmask = ctx->d_wmask;
@@ -431,7 +512,7 @@ epi_status launch_run(epi_ctx *ctx, ScanRun &r)
     if (r.ntiles > 0) {
         const int grid = (int)std::min<int64_t>(r.ntiles, ctx->sm_count);
         if (r.form == EPI_FORM_TENSOR) {
-            CK(epi::launch_mma(r.args, grid, ctx->stream));
+            CK(epi::launch_mma(r.args, ctx->maps, grid, ctx->stream));
         } else {
             CK(epi::launch_popc(r.args, grid, ctx->stream));
         }
@@ -475,8 +556,13 @@ extern "C" epi_status epi_scan(epi_ctx *ctx, const epi_block *blocks, int32_t nb
         r.args.cap = ctx->hit_cap;
         s = launch_run(ctx, r);
         if (s != EPI_OK) return s;
-        CK(cudaMemcpyAsync(&found, ctx->d_counters, sizeof(found), cudaMemcpyDeviceToHost, ctx->stream));
+        unsigned long long cnt[4];
+        CK(cudaMemcpyAsync(cnt, ctx->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        if (cnt[2] != 0)
+            return set_err(ctx, EPI_E_TIMEOUT, "a bounded device wait of the scan kernel gave up (site %llu)",
+                           cnt[3]);
+        found = cnt[0];
         if ((int64_t)found <= ctx->hit_cap) break;
         // every hit is needed to put the first `cap` in output order: grow and rescan
         cudaFree(ctx->d_hits);
@@ -587,6 +673,13 @@ extern "C" epi_status epi_scan_dump(epi_ctx *ctx, const epi_block *block, const 
         r.args.hits = ctx->d_hits;
         r.args.cap = 0;
         st = launch_run(ctx, r);
+    }
+    if (st == EPI_OK) {
+        unsigned long long cnt[4];
+        cudaError_t e = cudaMemcpyAsync(cnt, ctx->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) st = set_err(ctx, EPI_E_CUDA, "dump: %s", cudaGetErrorString(e));
+        else if (cnt[2] != 0) st = set_err(ctx, EPI_E_TIMEOUT, "a bounded device wait gave up (site %llu)", cnt[3]);
     }
     if (st == EPI_OK) {
         for (Out &x : outs) {

@@ -8,9 +8,19 @@
 //   y       float [T][Np]         trait column centred by its valid mean, 0 where invalid
 //   q       float [T][Np]         y^2 - qc[t] (qc = mean of y^2 over valid), 0 where invalid
 //   wmask   uint32 [T][Wp]        phenotype-valid bits
-// Individuals are padded to Np = 32*Wp; padding carries no genotype and no phenotype.
+// and for the tensor-core form
+//   hcodes  uint8 [nsnp][Np]      one-hot genotype byte: 1 << g for g in 0..2, 0 if missing
+//   missbits uint32 [nsnp][Wp]    missing-genotype bits; misssum [nsnp][Ws] marks non-zero words
+//   ydig    int8 [T][4][Np]       per individual: phenotype-valid flag and the three balanced
+//                                 base-256 digits (low first) of round(y * 2^sy)
+//   qd      double [T][Np]        (quantised y)^2, 0 where invalid; qtot[T] its sum;
+//   qm      double [T][nsnp]      the part of qtot on individuals missing at that SNP
+// Individuals are padded to Np = 32*Wp (a multiple of 128); padding carries no genotype
+// and no phenotype.
 #pragma once
 #include <cstdint>
+#include <cstring>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace epi {
@@ -34,14 +44,16 @@ struct ScanArgs {
     // genotypes
     const uint4 *planes;
     const uint32_t *codes;
-    int32_t Wp, Wc, nid;
+    const uint8_t *hcodes;
+    const uint32_t *missbits, *misssum;
+    int32_t Wp, Wc, Ws, nid, nsnp;
     // traits
     const float *y, *q;
     const uint32_t *wmask;
     const double *qc;          // [T]
     const double *yscale;      // [T] (tensor form: 2^-sy)
-    const double *qscale;      // [T]
-    const int8_t *ydig;        // tensor form digit planes (see scan_mma.cu)
+    const double *qd, *qtot, *qm;
+    const int8_t *ydig;
     int32_t Np, ntraits;
     // blocks / tiles
     const BlockDesc *blocks;
@@ -53,12 +65,17 @@ struct ScanArgs {
     // outputs
     DevHit *hits;
     int64_t cap;
-    unsigned long long *counters;  // [0] hits found, [1] tile queue
+    unsigned long long *counters;  // [0] hits found, [1] tile queue, [2] error flag, [3] error site
     unsigned int *maxf, *maxf2;    // [T] order-preserving encoded floats
     // optional dump of one block (pair (gx, gy) at gx*size2 + gy)
     int32_t *dump_counts;
     float *dump_F, *dump_F2;
     int32_t *dump_df1, *dump_df2;
+};
+
+// TMA descriptors of the tensor form (kernel parameter, __grid_constant__)
+struct MmaMaps {
+    CUtensorMap hi, hj, dg;
 };
 
 // float -> unsigned with the same order (for atomicMax over possibly negative F)

@@ -19,40 +19,101 @@ __device__ __forceinline__ uint32_t ref_code(const int32_t *row, int k, int nid,
     return ((uint32_t)row[npack] >> (2 * (remain - 1 - t))) & 3u;
 }
 
-// One thread per (SNP, 32-individual word).
+// One thread per (SNP, 32-individual word). Also writes the tensor form's one-hot code
+// bytes (1 << g, 0 when missing or padding) and missing-genotype bits.
 __global__ void k_unpack(const int32_t *__restrict__ raw, int nsnp, int nid, int npack, int remain,
-                         int npack1, uint4 *__restrict__ planes, int Wp, uint32_t *__restrict__ codes, int Wc)
+                         int npack1, uint4 *__restrict__ planes, int Wp, uint32_t *__restrict__ codes, int Wc,
+                         uint8_t *__restrict__ hcodes, uint32_t *__restrict__ missbits)
 {
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long total = (long long)nsnp * Wp;
     if (gid >= total) return;
     const int s = (int)(gid / Wp), w = (int)(gid % Wp);
     const int32_t *row = raw + (size_t)s * npack1;
-    uint32_t p0 = 0, p1 = 0, p2 = 0, c0 = 0, c1 = 0;
-#pragma unroll 4
+    uint32_t p0 = 0, p1 = 0, p2 = 0, c0 = 0, c1 = 0, miss = 0;
+    uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
     for (int t = 0; t < 32; ++t) {
-        const uint32_t c = ref_code(row, 32 * w + t, nid, npack, remain);
+        const int k = 32 * w + t;
+        const uint32_t c = ref_code(row, k, nid, npack, remain);
         p0 |= (uint32_t)(c == 0u) << t;
         p1 |= (uint32_t)(c == 1u) << t;
         p2 |= (uint32_t)(c == 2u) << t;
+        miss |= (uint32_t)(c == 3u && k < nid) << t;
+        h[t >> 2] |= (c < 3u ? (1u << c) : 0u) << (8 * (t & 3));
         if (t < 16) c0 |= c << (2 * t);
         else c1 |= c << (2 * (t - 16));
     }
     planes[(size_t)s * Wp + w] = make_uint4(p0, p1, p2, p0 | p1 | p2);
+    if (hcodes != nullptr) {
+        uint4 *dst = reinterpret_cast<uint4 *>(hcodes + ((size_t)s * Wp + w) * 32);
+        dst[0] = make_uint4(h[0], h[1], h[2], h[3]);
+        dst[1] = make_uint4(h[4], h[5], h[6], h[7]);
+    }
+    if (missbits != nullptr) missbits[(size_t)s * Wp + w] = miss;
     if (codes != nullptr) {
         if (2 * w < Wc) codes[(size_t)s * Wc + 2 * w] = c0;
         if (2 * w + 1 < Wc) codes[(size_t)s * Wc + 2 * w + 1] = c1;
     }
 }
 
+// Per SNP: bit w' of summary word s marks a non-zero missing word 32 s + w'.
+__global__ void k_misssum(const uint32_t *__restrict__ missbits, int nsnp, int Wp, uint32_t *__restrict__ misssum,
+                          int Ws)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)nsnp * Ws) return;
+    const int s = (int)(gid / Ws), q = (int)(gid % Ws);
+    uint32_t m = 0;
+    for (int b = 0; b < 32; ++b) {
+        const int w = 32 * q + b;
+        if (w < Wp && missbits[(size_t)s * Wp + w] != 0u) m |= 1u << b;
+    }
+    misssum[gid] = m;
+}
+
+// qm[t][s] = sum over individuals missing at SNP s (and phenotype-valid for t) of qd[t][k]
+__global__ void k_qmiss(const uint32_t *__restrict__ missbits, int nsnp, int Wp, const uint32_t *__restrict__ wmask,
+                        const double *__restrict__ qd, int Np, int ntraits, double *__restrict__ qm)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)nsnp * ntraits) return;
+    const int t = (int)(gid / nsnp), s = (int)(gid % nsnp);
+    double x = 0.0;
+    const uint32_t *mb = missbits + (size_t)s * Wp;
+    for (int w = 0; w < Wp; ++w) {
+        uint32_t bits = mb[w] & wmask[(size_t)t * Wp + w];
+        while (bits) {
+            x += qd[(size_t)t * Np + 32 * w + __ffs(bits) - 1];
+            bits &= bits - 1;
+        }
+    }
+    qm[gid] = x;
+}
+
 cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int remain, uint4 *planes, int Wp,
-                          uint32_t *codes, int Wc, cudaStream_t stream)
+                          uint32_t *codes, int Wc, uint8_t *hcodes, uint32_t *missbits, uint32_t *misssum, int Ws,
+                          cudaStream_t stream)
 {
     const int npack1 = remain ? npack + 1 : npack;
     const long long total = (long long)nsnp * Wp;
     const int nt = 256;
     const long long nb = (total + nt - 1) / nt;
-    k_unpack<<<(unsigned)nb, nt, 0, stream>>>(raw, nsnp, nid, npack, remain, npack1, planes, Wp, codes, Wc);
+    k_unpack<<<(unsigned)nb, nt, 0, stream>>>(raw, nsnp, nid, npack, remain, npack1, planes, Wp, codes, Wc, hcodes,
+                                              missbits);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || misssum == nullptr) return e;
+    const long long t2 = (long long)nsnp * Ws;
+    k_misssum<<<(unsigned)((t2 + nt - 1) / nt), nt, 0, stream>>>(missbits, nsnp, Wp, misssum, Ws);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_qmiss(const uint32_t *missbits, int nsnp, int Wp, const uint32_t *wmask, const double *qd, int Np,
+                         int ntraits, double *qm, cudaStream_t stream)
+{
+    const long long total = (long long)nsnp * ntraits;
+    const int nt = 256;
+    k_qmiss<<<(unsigned)((total + nt - 1) / nt), nt, 0, stream>>>(missbits, nsnp, Wp, wmask, qd, Np, ntraits, qm);
     return cudaGetLastError();
 }
 

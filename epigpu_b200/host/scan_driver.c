@@ -17,11 +17,15 @@
  *  - hits are counted with atomics and returned in the reference's serial order instead
  *    of 200-row slots written without synchronisation (EpiOpenCL.c:253-255), so no hit is
  *    lost or overwritten whatever the count;
+ *  - a results file cut inside a block (interrupted write) is truncated back to the end of
+ *    its last complete block before the scan resumes; the reference appends after the
+ *    partial rows;
  *  - errors print the library's message and exit with its status (ereport, :1159-1177).
  */
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #include "epigpu_host.h"
 
@@ -82,6 +86,7 @@ int resume_point(const char *filename, int *chr1, int *chr2, int *tothits, int n
         return 1;
     }
     /* count complete blocks: a block header followed by all of its rows */
+    long good_end = ftell(in);
     while (fgets(line, sizeof(line), in)) {
         int a, b, n;
         if (sscanf(line, "# %d x %d : %d interactions", &a, &b, &n) != 3) break;
@@ -93,8 +98,15 @@ int resume_point(const char *filename, int *chr1, int *chr2, int *tothits, int n
         k = n;
         *tothits += k;
         ++blocks;
+        good_end = ftell(in);
     }
+    fseek(in, 0, SEEK_END);
+    const long size = ftell(in);
     fclose(in);
+    if (blocks && size > good_end && truncate(filename, good_end) != 0) {
+        printf("Cannot truncate the partial block at the end of %s\n", filename);
+        exit(1);
+    }
     if (blocks) {
         if (c1 == c2) {
             *chr1 = c1 + 1;

@@ -10,7 +10,7 @@ def pair_key(h):
 
 def near_threshold(b_per_pair, block, t1, t2, test, tol):
     """Pairs (global snp1, snp2) whose FP64 F (or F2) lies within relative `tol` of its
-    threshold, plus pairs with df1 == 0 (F is 0/0 in exact arithmetic; the reference's
+    threshold, plus pairs with df1 <= 0 (F is 0/0 in exact arithmetic; the reference's
     float32 gives NaN or inf there depending on rounding)."""
     s1, m1, s2, m2 = block
     F, F2, d1 = b_per_pair["F"], b_per_pair["F2"], b_per_pair["df1"]
@@ -18,7 +18,7 @@ def near_threshold(b_per_pair, block, t1, t2, test, tol):
         near = np.abs(F - t1) <= tol * abs(t1)
         if test == "i":
             near |= np.abs(F2 - t2) <= tol * abs(t2)
-    near |= (d1 == 0)
+    near |= (d1 <= 0)
     gx, gy = np.nonzero(near)
     return set(zip((gx + s1).tolist(), (gy + s2).tolist()))
 

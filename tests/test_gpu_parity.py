@@ -17,7 +17,8 @@ pytestmark = pytest.mark.gpu
 
 F_TOL = 1e-5      # F / F2 relative error against the FP64 oracle
 TOL_SET = 1e-4    # threshold neighbourhood excluded from the hit-set comparison
-FORMS = [capi.FORM_POPC]
+FORMS = [capi.FORM_POPC, capi.FORM_TENSOR]
+FORM_IDS = ["popc", "tensor"]
 
 
 def _data(nid, nsnp, seed, miss_g=0.01, miss_p=0.02):
@@ -71,7 +72,7 @@ def _check_block(ctx, codes, gp, phen, block, test, safe, t1, t2, form, chunk=12
     return got
 
 
-@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
 @pytest.mark.parametrize("test,safe", [("f", 0), ("i", 0), ("f", 1), ("i", 1)])
 def test_single_chromosome(gpu_ctx, form, test, safe):
     codes, gp, phen = _data(500, 400, seed=21)
@@ -81,7 +82,7 @@ def test_single_chromosome(gpu_ctx, form, test, safe):
     assert len(got) > 0
 
 
-@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
 def test_all_pairs_threshold_off(gpu_ctx, form):
     """Threshold -inf: every pair with a finite F is a hit, in reference order."""
     codes, gp, phen = _data(333, 250, seed=5)
@@ -89,7 +90,7 @@ def test_all_pairs_threshold_off(gpu_ctx, form):
     assert len(got) > 20000
 
 
-@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
 @pytest.mark.parametrize("nid", [7, 16, 31, 32, 33, 100, 129])
 def test_ragged_individuals(gpu_ctx, form, nid):
     """remain-only, remain == 0 and word-boundary individual counts (readplink.c:1090-1098)."""
@@ -97,7 +98,7 @@ def test_ragged_individuals(gpu_ctx, form, nid):
     _check_block(gpu_ctx, codes, gp, phen, (0, 90, 0, 90), "i", 0, 1.0, 1.0, form)
 
 
-@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
 def test_uneven_chromosomes(gpu_ctx, form):
     """Three chromosome blocks of uneven sizes in perform_scan's (i, j <= i) order."""
     sizes = [70, 131, 45]
@@ -126,7 +127,7 @@ def test_uneven_chromosomes(gpu_ctx, form):
     assert off == total
 
 
-@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
 def test_monomorphic_and_missing_snps(gpu_ctx, form):
     """All-one-genotype SNPs (nfac small, df1 == 0 pairs) and an all-missing SNP."""
     nid, nsnp = 120, 40
@@ -142,7 +143,7 @@ def test_monomorphic_and_missing_snps(gpu_ctx, form):
     assert not bad, "an all-missing SNP cannot produce a finite F"
 
 
-@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
 def test_chunk_order(gpu_ctx, form):
     """The -i iteration size changes the output order exactly as in the reference."""
     codes, gp, phen = _data(200, 300, seed=3)
@@ -150,7 +151,7 @@ def test_chunk_order(gpu_ctx, form):
         _check_block(gpu_ctx, codes, gp, phen, (0, 300, 0, 300), "f", 0, 2.0, 0, form, chunk=chunk)
 
 
-@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
 def test_overflow_reports_total(gpu_ctx, form):
     codes, gp, phen = _data(100, 120, seed=4)
     gpu_ctx.load_packed(gp, 100)
