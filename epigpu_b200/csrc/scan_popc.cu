@@ -2,35 +2,36 @@
 // (src/EpiOpenCL.c:110-228: unpack two SNPs, count the 3x3 genotype cells, add the
 // phenotype into its cell) redone for the B200's CUDA cores.
 //
-// Persistent kernel, one 256-thread CTA per SM, pulling 32 x 64 SNP-pair tiles from a
+// Persistent kernel, one 512-thread CTA per SM, pulling 64 x 32 SNP-pair tiles from a
 // queue over the triangular schedule of chromosome blocks. Per tile and trait it walks the
 // individuals in stages of 64:
-//   * stage expansion: the i-tile's bit-planes become U_a = [g_i==a]*y and U_V = [g_i valid],
-//     the j-tile's become F_b = [g_j==b] and F_Q = [g_j valid]*q, as floats in shared memory;
+//   * stage expansion: the i-tile's bit-planes become U_a = [g_i==a]*y and U_V = [g_i valid]
+//     as floats in shared memory (read by the whole warp: broadcast loads);
 //   * cell counts: AND + __popc of 32-bit plane words (phenotype mask folded into the
 //     i side), 16-bit packed counters;
-//   * cell sums: S_ab += U_a*F_b (9 FP32 FMAs per pair and individual) and
-//     Q += U_V*F_Q (sum of y^2 over valid individuals, with q = y^2 - mean y^2).
-// Each thread owns 4 x 2 whole pairs (no cross-lane reduction needed); the warp's four
-// i-SNPs are shared (broadcast loads), each lane has its own two j-SNPs.
+//   * cell sums: each lane turns its own j-SNP's plane bits into F_b = [g_j==b] and
+//     F_Q = [g_j valid]*q in registers, then S_ab += U_a*F_b (9 FP32 FMAs per pair and
+//     individual) and Q += U_V*F_Q (sum of y^2 over valid individuals, q = y^2 - mean y^2).
+// Each thread owns 4 whole pairs (the warp's four i-SNPs x the lane's j-SNP): no
+// cross-lane reduction; ~100 registers so 16 warps per SM hide shared-memory latency.
 // Epilogue: FP64 SSB/SSI/F/F2 per pair, warp-aggregated atomic hit append, per-trait max F.
 #include "epi_internal.cuh"
 
 namespace epi {
 namespace popc {
 
-constexpr int TI = 32;   // i-SNPs per tile (8 warps x 4)
-constexpr int TJ = 64;   // j-SNPs per tile (32 lanes x 2)
-constexpr int NT = 256;
+constexpr int TI = 64;   // i-SNPs per tile (16 warps x 4, shared by the warp's lanes)
+constexpr int TJ = 32;   // j-SNPs per tile (one per lane)
+constexpr int NT = 512;
 constexpr int KI = 64;   // individuals per stage
 constexpr int KW = 2;    // 32-individual words per stage
 constexpr int KP = 32;   // individual pairs per stage
 
 struct __align__(16) Smem {
     float4 u[KP][2][TI];  // [0] = (U0a, U0b, U1a, U1b), [1] = (U2a, U2b, UVa, UVb)
-    float4 f[KP][2][TJ];  // [0] = (F0a, F0b, F1a, F1b), [1] = (F2a, F2b, FQa, FQb)
     uint4 pi[KW][TI];     // i-side planes AND phenotype mask
     uint4 pj[KW][TJ];     // j-side planes
+    float2 q[KP];         // q of the two individuals of each pair
     long long tile;
 };
 
@@ -46,31 +47,15 @@ __device__ __forceinline__ void count9(uint32_t c[5], const uint4 &p, const uint
     c[4] += __popc(p.z & r.z);
 }
 
-__device__ __forceinline__ void fma_pair(float s[9], float &q, const float4 &ua, const float4 &ub,
-                                         const float4 &fa, const float4 &fb)
-{
-    const float U[3][2] = {{ua.x, ua.y}, {ua.z, ua.w}, {ub.x, ub.y}};
-    const float Fv[3][2] = {{fa.x, fa.y}, {fa.z, fa.w}, {fb.x, fb.y}};
-#pragma unroll
-    for (int x = 0; x < 3; ++x)
-#pragma unroll
-        for (int y = 0; y < 3; ++y) {
-            s[3 * x + y] = fmaf(U[x][0], Fv[y][0], s[3 * x + y]);
-            s[3 * x + y] = fmaf(U[x][1], Fv[y][1], s[3 * x + y]);
-        }
-    q = fmaf(ub.z, fb.z, q);
-    q = fmaf(ub.w, fb.w, q);
-}
-
-// FP64 statistics of one pair from its packed counts, FP32 cell sums and y^2 sum; also
-// writes the optional per-pair dump. Kept out of line: the kernel's accumulators stay in
-// registers and only this call's arguments go through the stack.
 struct PairAcc {
     uint32_t C[5];
     float S[9];
     float Q;
 };
 
+// FP64 statistics of one pair from its packed counts, FP32 cell sums and y^2 sum; also
+// writes the optional per-pair dump. Kept out of line: the kernel's accumulators stay in
+// registers and only this call's arguments go through the stack.
 __device__ __noinline__ PairStat eval_pair(const ScanArgs &a, const PairAcc acc, double qc, int t, int gi, int gj,
                                            int size2)
 {
@@ -121,19 +106,17 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
             const float *yt = a.y + (size_t)t * a.Np;
             const float *qt = a.q + (size_t)t * a.Np;
             const uint32_t *wt = a.wmask + (size_t)t * a.Wp;
-            float S[4][2][9];
-            float Q[4][2];
-            uint32_t C[4][2][5];
+            float S[4][9];
+            float Q[4];
+            uint32_t C[4][5];
 #pragma unroll
-            for (int ii = 0; ii < 4; ++ii)
+            for (int ii = 0; ii < 4; ++ii) {
 #pragma unroll
-                for (int jj = 0; jj < 2; ++jj) {
+                for (int c = 0; c < 9; ++c) S[ii][c] = 0.0f;
+                Q[ii] = 0.0f;
 #pragma unroll
-                    for (int c = 0; c < 9; ++c) S[ii][jj][c] = 0.0f;
-                    Q[ii][jj] = 0.0f;
-#pragma unroll
-                    for (int c = 0; c < 5; ++c) C[ii][jj][c] = 0u;
-                }
+                for (int c = 0; c < 5; ++c) C[ii][c] = 0u;
+            }
 
             for (int st = 0; st < nstages; ++st) {
                 const int w0 = st * KW, k0 = st * KI;
@@ -157,28 +140,6 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
                                                                bitf(P.w, bA), bitf(P.w, bB));
                     }
                 }
-                {   // j side: thread -> (j, 16 individuals)
-                    const int j = tid >> 2, part = tid & 3;
-                    const int gj = j0 + j;
-                    uint4 P = make_uint4(0, 0, 0, 0);
-                    if (gj < bd.size2) P = a.planes[(size_t)(bd.start2 + gj) * a.Wp + w0 + (part >> 1)];
-                    const int bit0 = 16 * (part & 1);
-#pragma unroll
-                    for (int h = 0; h < 4; ++h) {
-                        const float4 qv = *reinterpret_cast<const float4 *>(qt + k0 + 16 * part + 4 * h);
-                        const float qq[4] = {qv.x, qv.y, qv.z, qv.w};
-#pragma unroll
-                        for (int e2 = 0; e2 < 2; ++e2) {
-                            const int e = 2 * h + e2;
-                            const int bA = bit0 + 2 * e, bB = bA + 1;
-                            sm.f[part * 8 + e][0][j] = make_float4(bitf(P.x, bA), bitf(P.x, bB),
-                                                                   bitf(P.y, bA), bitf(P.y, bB));
-                            sm.f[part * 8 + e][1][j] = make_float4(bitf(P.z, bA), bitf(P.z, bB),
-                                                                   bitsel(P.w, bA, qq[2 * e2]),
-                                                                   bitsel(P.w, bB, qq[2 * e2 + 1]));
-                        }
-                    }
-                }
                 if (tid < KW * TI) {
                     const int w = tid / TI, i = tid % TI, gi = i0 + i;
                     uint4 P = make_uint4(0, 0, 0, 0);
@@ -190,28 +151,44 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
                     uint4 P = make_uint4(0, 0, 0, 0);
                     if (gj < bd.size2) P = a.planes[(size_t)(bd.start2 + gj) * a.Wp + w0 + w];
                     sm.pj[w][j] = P;
+                } else if (tid < KW * TI + KW * TJ + KP) {
+                    const int kp = tid - KW * TI - KW * TJ;
+                    sm.q[kp] = *reinterpret_cast<const float2 *>(qt + k0 + 2 * kp);
                 }
                 __syncthreads();
 
 #pragma unroll
                 for (int w = 0; w < KW; ++w) {
-                    const uint4 r0 = sm.pj[w][lane], r1 = sm.pj[w][lane + 32];
+                    const uint4 r = sm.pj[w][lane];
 #pragma unroll
-                    for (int ii = 0; ii < 4; ++ii) {
-                        const uint4 p = sm.pi[w][warp * 4 + ii];
-                        count9(C[ii][0], p, r0);
-                        count9(C[ii][1], p, r1);
-                    }
+                    for (int ii = 0; ii < 4; ++ii) count9(C[ii], sm.pi[w][warp * 4 + ii], r);
                 }
-#pragma unroll 2
-                for (int kp = 0; kp < KP; ++kp) {
-                    const float4 fa0 = sm.f[kp][0][lane], fb0 = sm.f[kp][1][lane];
-                    const float4 fa1 = sm.f[kp][0][lane + 32], fb1 = sm.f[kp][1][lane + 32];
 #pragma unroll
-                    for (int ii = 0; ii < 4; ++ii) {
-                        const float4 ua = sm.u[kp][0][warp * 4 + ii], ub = sm.u[kp][1][warp * 4 + ii];
-                        fma_pair(S[ii][0], Q[ii][0], ua, ub, fa0, fb0);
-                        fma_pair(S[ii][1], Q[ii][1], ua, ub, fa1, fb1);
+                for (int w = 0; w < KW; ++w) {
+                    // this lane's j-SNP: indicator floats from its plane bits
+                    const uint4 r = sm.pj[w][lane];
+#pragma unroll 1
+                    for (int h = 0; h < 16; ++h) {
+                        const int kp = 16 * w + h, bA = 2 * h, bB = bA + 1;
+                        const float2 qq = sm.q[kp];
+                        const float F[3][2] = {{bitf(r.x, bA), bitf(r.x, bB)},
+                                               {bitf(r.y, bA), bitf(r.y, bB)},
+                                               {bitf(r.z, bA), bitf(r.z, bB)}};
+                        const float FQa = bitsel(r.w, bA, qq.x), FQb = bitsel(r.w, bB, qq.y);
+#pragma unroll
+                        for (int ii = 0; ii < 4; ++ii) {
+                            const float4 ua = sm.u[kp][0][warp * 4 + ii], ub = sm.u[kp][1][warp * 4 + ii];
+                            const float U[3][2] = {{ua.x, ua.y}, {ua.z, ua.w}, {ub.x, ub.y}};
+#pragma unroll
+                            for (int x = 0; x < 3; ++x)
+#pragma unroll
+                                for (int y = 0; y < 3; ++y) {
+                                    S[ii][3 * x + y] = fmaf(U[x][0], F[y][0], S[ii][3 * x + y]);
+                                    S[ii][3 * x + y] = fmaf(U[x][1], F[y][1], S[ii][3 * x + y]);
+                                }
+                            Q[ii] = fmaf(ub.z, FQa, Q[ii]);
+                            Q[ii] = fmaf(ub.w, FQb, Q[ii]);
+                        }
                     }
                 }
             }
@@ -220,9 +197,8 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
             const double qc = a.qc[t];
             const bool report = a.report_trait < 0 || a.report_trait == t;
 #pragma unroll
-            for (int p = 0; p < 8; ++p) {
-                const int ii = p >> 1, jj = p & 1;
-                const int gi = i0 + warp * 4 + ii, gj = j0 + lane + 32 * jj;
+            for (int ii = 0; ii < 4; ++ii) {
+                const int gi = i0 + warp * 4 + ii, gj = j0 + lane;
                 const bool valid = gi < bd.size1 && gj < bd.size2 && (bd.start1 + gi > bd.start2 + gj);
                 PairStat s;
                 s.nfac = s.d1 = s.d2 = 0;
@@ -230,10 +206,10 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
                 if (valid) {
                     PairAcc acc;
 #pragma unroll
-                    for (int c = 0; c < 5; ++c) acc.C[c] = C[ii][jj][c];
+                    for (int c = 0; c < 5; ++c) acc.C[c] = C[ii][c];
 #pragma unroll
-                    for (int c = 0; c < 9; ++c) acc.S[c] = S[ii][jj][c];
-                    acc.Q = Q[ii][jj];
+                    for (int c = 0; c < 9; ++c) acc.S[c] = S[ii][c];
+                    acc.Q = Q[ii];
                     s = eval_pair(a, acc, qc, t, gi, gj, bd.size2);
                 }
                 const bool hit = valid && report && is_hit(a, s);

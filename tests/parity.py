@@ -47,13 +47,16 @@ def kappa(F, df1, df2):
 
 
 def f_excess(got, ref, df1, df2, tol):
-    """Relative error of F against the FP64 oracle divided by its allowed bound
-    tol*kappa; <= 1 passes. NaN/zero references are skipped (returned as 0)."""
+    """Error of F against the FP64 oracle divided by its allowed bound
+    tol * kappa * max(|F|, 1): relative for F >= 1 (every threshold region), absolute for
+    F < 1 where a relative error has no meaning as F -> 0. <= 1 passes. NaN references
+    (no valid individual, df1 <= 0) are skipped (returned as 0)."""
     got = np.asarray(got, dtype=np.float64)
     ref = np.asarray(ref, dtype=np.float64)
-    ok = np.isfinite(ref) & (np.abs(ref) > 0) & (np.asarray(df1) > 0) & (np.asarray(df2) > 0)
+    ok = np.isfinite(ref) & (np.asarray(df1) > 0) & (np.asarray(df2) > 0)
     out = np.zeros(ref.shape)
-    out[ok] = oracles.rel_err(got[ok], ref[ok]) / (tol * kappa(ref[ok], np.asarray(df1)[ok], np.asarray(df2)[ok]))
+    err = np.abs(got[ok] - ref[ok]) / np.maximum(np.abs(ref[ok]), 1.0)
+    out[ok] = err / (tol * kappa(ref[ok], np.asarray(df1)[ok], np.asarray(df2)[ok]))
     return out
 
 

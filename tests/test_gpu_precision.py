@@ -1,7 +1,8 @@
 """F accuracy at the headline's individual count (N = 10,000): both GPU forms against
 the FP64 oracle on every pair of a seeded 600-SNP block (179,700 pairs), 8 df and 4 df.
-Reports max and median relative error; the bar is 1e-5 (times kappa = SSY/SSW, which is
-~1 at this N). Cell counts must match exactly on every pair."""
+Reports max and median relative error over the pairs with F >= 1 and the max absolute
+error below; the bar is 1e-5 relative (absolute under F = 1; times kappa = SSY/SSW, ~1 at
+this N). Cell counts must match exactly on every pair."""
 import numpy as np
 import pytest
 
@@ -37,9 +38,12 @@ def test_f_error_at_n10000(gpu_ctx, data, form):
     for field in ("F", "F2"):
         ref = pb[field][tri]
         got = d[field][tri].astype(np.float64)
-        err = oracles.rel_err(got, ref)
-        out[field] = (float(err.max()), float(np.median(err)))
+        big = np.abs(ref) >= 1.0
+        rel = oracles.rel_err(got[big], ref[big])
+        absl = np.abs(got[~big] - ref[~big])
+        out[field] = (float(rel.max()), float(np.median(rel)), int(big.sum()), float(absl.max()))
         assert parity.f_excess(got, ref, pb["df1"][tri], pb["df2"][tri], 1e-5).max() <= 1.0
-        assert err.max() <= 1e-5
-    print("\nF error vs FP64, form %d, N=%d, %d pairs: 8df max %.3g median %.3g; 4df max %.3g median %.3g"
-          % (form, NID, tri.sum(), out["F"][0], out["F"][1], out["F2"][0], out["F2"][1]))
+        assert rel.max() <= 1e-5 and absl.max() <= 1e-5
+    print("\nF error vs FP64, form %d, N=%d, %d pairs: 8df rel max %.3g median %.3g (%d pairs F>=1), abs max "
+          "%.3g below; 4df rel max %.3g median %.3g (%d pairs), abs max %.3g below"
+          % (form, NID, tri.sum(), *out["F"], *out["F2"]))
