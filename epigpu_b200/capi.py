@@ -27,7 +27,7 @@ FORM_AUTO, FORM_POPC, FORM_TENSOR = 0, 1, 2
 EXPORTS = (
     "epi_default_opts", "epi_open", "epi_close", "epi_strerror", "epi_last_error",
     "epi_device_info", "epi_load_packed", "epi_set_traits", "epi_set_phenotype", "epi_scan",
-    "epi_scan_dump", "epi_last_timing", "epi_get_stream", "epi_permute_phenotype",
+    "epi_scan_dump", "epi_last_timing", "epi_get_stream", "epi_scan_block_noalloc", "epi_permute_phenotype",
 )
 
 
@@ -69,6 +69,8 @@ _SIGS = {
     "epi_last_timing": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64),
                                        ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
     "epi_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+    "epi_scan_block_noalloc": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _P, ctypes.POINTER(Block),
+                                              ctypes.POINTER(ScanOpts), _P, ctypes.c_int64, _P, _P, _P]),
     "epi_permute_phenotype": (None, [_P, ctypes.c_int32, ctypes.c_uint32]),
 }
 

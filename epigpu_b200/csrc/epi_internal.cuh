@@ -40,6 +40,13 @@ struct BlockDesc {
     int64_t tile_base;
 };
 
+// The reference's 24-byte result row (src/id4117.h:14-21), as written on the device by the
+// allocation-free entry point.
+struct HitRow {
+    int32_t snp1, snp2, df1, df2;
+    float F, F2;
+};
+
 struct ScanArgs {
     // genotypes
     const uint4 *planes;
@@ -71,7 +78,13 @@ struct ScanArgs {
     int32_t *dump_counts;
     float *dump_F, *dump_F2;
     int32_t *dump_df1, *dump_df2;
+    // allocation-free entry point only: genotypes read straight from the reference's
+    // packed words, hits written as 24-byte result rows
+    const int32_t *gpack;
+    int32_t npack, remain;
+    HitRow *rows;
 };
+
 
 // TMA descriptors of the tensor form (kernel parameter, __grid_constant__)
 struct MmaMaps {
@@ -185,6 +198,31 @@ __device__ __forceinline__ void emit_hit(const ScanArgs &a, bool hit, int snp1, 
             h.trait = trait;
             h.block = block;
             a.hits[idx] = h;
+        }
+    }
+}
+
+// Warp-aggregated append of 24-byte result rows (allocation-free entry point).
+__device__ __forceinline__ void emit_row(const ScanArgs &a, bool hit, int snp1, int snp2, const PairStat &s)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned mask = __ballot_sync(0xffffffffu, hit);
+    if (mask == 0u) return;
+    const int leader = __ffs(mask) - 1;
+    unsigned long long base = 0;
+    if ((int)lane == leader) base = atomicAdd(&a.counters[0], (unsigned long long)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (hit) {
+        const unsigned long long idx = base + __popc(mask & ((1u << lane) - 1u));
+        if ((long long)idx < a.cap) {
+            HitRow h;
+            h.snp1 = snp1;
+            h.snp2 = snp2;
+            h.df1 = s.d1;
+            h.df2 = s.d2;
+            h.F = (float)s.F;
+            h.F2 = a.test_int ? (float)s.F2 : 0.0f;
+            a.rows[idx] = h;
         }
     }
 }

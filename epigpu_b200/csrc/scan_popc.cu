@@ -16,6 +16,7 @@
 // cross-lane reduction; ~100 registers so 16 warps per SM hide shared-memory latency.
 // Epilogue: FP64 SSB/SSI/F/F2 per pair, warp-aggregated atomic hit append, per-trait max F.
 #include "epi_internal.cuh"
+#include "epigpu.h"
 
 namespace epi {
 namespace popc {
@@ -45,6 +46,29 @@ __device__ __forceinline__ void count9(uint32_t c[5], const uint4 &p, const uint
     c[2] += __popc(p.y & r.y) + (__popc(p.y & r.z) << 16);
     c[3] += __popc(p.z & r.x) + (__popc(p.z & r.y) << 16);
     c[4] += __popc(p.z & r.z);
+}
+
+// Genotype bit-planes of 32 individuals (word w) of one SNP: from the library's plane array,
+// or, in the allocation-free variant, decoded straight from the reference's packed row
+// (src/readplink.c:1066-1102: MSB-first words, right-aligned tail word).
+template <bool RAW>
+__device__ __forceinline__ uint4 load_planes(const ScanArgs &a, int snp, int w)
+{
+    if (!RAW) return a.planes[(size_t)snp * a.Wp + w];
+    const int npack1 = a.remain ? a.npack + 1 : a.npack;
+    const uint32_t *row = reinterpret_cast<const uint32_t *>(a.gpack) + (size_t)snp * npack1;
+    uint32_t p0 = 0, p1 = 0, p2 = 0;
+#pragma unroll 4
+    for (int t = 0; t < 32; ++t) {
+        const int k = 32 * w + t;
+        uint32_t c = 3u;
+        if (k < 16 * a.npack) c = (__ldg(row + (k >> 4)) >> (30 - 2 * (k & 15))) & 3u;
+        else if (k < a.nid) c = (__ldg(row + a.npack) >> (2 * (a.remain - 1 - (k - 16 * a.npack)))) & 3u;
+        p0 |= (uint32_t)(c == 0u) << t;
+        p1 |= (uint32_t)(c == 1u) << t;
+        p2 |= (uint32_t)(c == 2u) << t;
+    }
+    return make_uint4(p0, p1, p2, p0 | p1 | p2);
 }
 
 struct PairAcc {
@@ -82,6 +106,9 @@ __device__ __noinline__ PairStat eval_pair(const ScanArgs &a, const PairAcc acc,
     return s;
 }
 
+// RAW = false: the library path (epi_scan). RAW = true: the allocation-free variant,
+// reading the reference's packed words and writing 24-byte rows (epi_scan_block_noalloc).
+template <bool RAW>
 __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -125,7 +152,7 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
                     const int i = tid >> 3, part = tid & 7;
                     const int gi = i0 + i;
                     uint4 P = make_uint4(0, 0, 0, 0);
-                    if (gi < bd.size1) P = a.planes[(size_t)(bd.start1 + gi) * a.Wp + w0 + (part >> 2)];
+                    if (gi < bd.size1) P = load_planes<RAW>(a, bd.start1 + gi, w0 + (part >> 2));
                     const float4 ya = *reinterpret_cast<const float4 *>(yt + k0 + 8 * part);
                     const float4 yb = *reinterpret_cast<const float4 *>(yt + k0 + 8 * part + 4);
                     const float yv[8] = {ya.x, ya.y, ya.z, ya.w, yb.x, yb.y, yb.z, yb.w};
@@ -143,13 +170,13 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
                 if (tid < KW * TI) {
                     const int w = tid / TI, i = tid % TI, gi = i0 + i;
                     uint4 P = make_uint4(0, 0, 0, 0);
-                    if (gi < bd.size1) P = a.planes[(size_t)(bd.start1 + gi) * a.Wp + w0 + w];
+                    if (gi < bd.size1) P = load_planes<RAW>(a, bd.start1 + gi, w0 + w);
                     const uint32_t W = wt[w0 + w];
                     sm.pi[w][i] = make_uint4(P.x & W, P.y & W, P.z & W, 0u);
                 } else if (tid < KW * TI + KW * TJ) {
                     const int idx = tid - KW * TI, w = idx / TJ, j = idx % TJ, gj = j0 + j;
                     uint4 P = make_uint4(0, 0, 0, 0);
-                    if (gj < bd.size2) P = a.planes[(size_t)(bd.start2 + gj) * a.Wp + w0 + w];
+                    if (gj < bd.size2) P = load_planes<RAW>(a, bd.start2 + gj, w0 + w);
                     sm.pj[w][j] = P;
                 } else if (tid < KW * TI + KW * TJ + KP) {
                     const int kp = tid - KW * TI - KW * TJ;
@@ -213,7 +240,8 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
                     s = eval_pair(a, acc, qc, t, gi, gj, bd.size2);
                 }
                 const bool hit = valid && report && is_hit(a, s);
-                emit_hit(a, hit, bd.start1 + gi, bd.start2 + gj, s, t, b);
+                if (RAW) emit_row(a, hit, bd.start1 + gi, bd.start2 + gj, s);
+                else emit_hit(a, hit, bd.start1 + gi, bd.start2 + gj, s, t, b);
                 fold_max(&a.maxf[t], valid, s.F);
                 if (a.test_int) fold_max(&a.maxf2[t], valid, s.F2);
             }
@@ -231,10 +259,216 @@ int popc_words_multiple() { return popc::KW; }
 cudaError_t launch_popc(const ScanArgs &a, int grid, cudaStream_t stream)
 {
     const size_t smem = sizeof(popc::Smem);
-    cudaError_t e = cudaFuncSetAttribute(popc::k_scan_popc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(popc::k_scan_popc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    popc::k_scan_popc<<<grid, popc::NT, smem, stream>>>(a);
+    popc::k_scan_popc<false><<<grid, popc::NT, smem, stream>>>(a);
     return cudaGetLastError();
 }
 
 }  // namespace epi
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free entry point (epi_scan_block_noalloc).
+//
+// Some callers cannot allocate GPU memory: code that must not call cudaMalloc while it runs
+// (a latency-critical service or a real-time loop after start-up), or a host framework
+// that hands out device memory only from its own pool. They pass device buffers for every
+// input and output, and the scan's working memory -- hit/tile counters, the block
+// descriptor, the per-trait maxima and the centred phenotype arrays -- lives in the fixed
+// array below, sized for at most EPI_NOALLOC_MAX_NID individuals (about 520 KiB, held by
+// every GPU that loads the library until the process exits).
+// ---------------------------------------------------------------------------------------
+namespace epi {
+namespace noalloc {
+
+constexpr int NP_MAX = 65536;  // individuals, padded to a multiple of 128
+
+struct Scratch {
+    unsigned long long counters[4];  // hits found, tile queue, error flag, error site
+    unsigned int maxf[2];            // order-encoded max F and max F2
+    double qc;                       // mean of the centred phenotype's square
+    BlockDesc block;
+    float y[NP_MAX];                 // centred phenotype (0 where missing)
+    float q[NP_MAX];                 // y^2 - qc (0 where missing)
+    uint32_t wmask[NP_MAX / 32];     // phenotype-valid bits
+};
+
+// The scratch: one copy per device, shared by every call on that device. In host code this
+// name only stands for the array; the device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_scratch[sizeof(Scratch)];
+
+__device__ __forceinline__ void block_sum(double &v, long long &n, double *sv, long long *sn)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) {
+        sv[w] = v;
+        sn[w] = n;
+    }
+    __syncthreads();
+    v = 0.0;
+    n = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+        v += sv[i];
+        n += sn[i];
+    }
+}
+
+// One block: resets the counters and maxima (every call starts from zero), writes the block
+// descriptor, then the centred phenotype as the library's epi_set_traits does on the host.
+__global__ void __launch_bounds__(1024) k_prep(Scratch *s, const float *__restrict__ phen, int nid, int Np, int Wp,
+                                               int safe, BlockDesc bd)
+{
+    __shared__ double sv[32];
+    __shared__ long long sn[32];
+    const int tid = threadIdx.x;
+    if (tid < 4) s->counters[tid] = 0ull;
+    if (tid < 2) s->maxf[tid] = 0x007fffffu;  // order-encoded -inf
+    if (tid == 0) s->block = bd;
+    double sum = 0.0;
+    long long n = 0;
+    for (int k = tid; k < nid; k += blockDim.x) {
+        const float y = phen[k];
+        if (safe || y != -9.0f) {
+            sum += (double)y;
+            ++n;
+        }
+    }
+    block_sum(sum, n, sv, sn);
+    const double mu = n ? sum / (double)n : 0.0;
+    double s2 = 0.0;
+    long long dummy = 0;
+    for (int k = tid; k < Np; k += blockDim.x) {
+        const float y = k < nid ? phen[k] : -9.0f;
+        const bool ok = k < nid && (safe || y != -9.0f);
+        const float yc = ok ? (float)((double)y - mu) : 0.0f;
+        s->y[k] = yc;
+        if (ok) s2 += (double)yc * (double)yc;
+    }
+    block_sum(s2, dummy, sv, sn);
+    const double c = n ? s2 / (double)n : 0.0;
+    if (tid == 0) s->qc = c;
+    for (int k = tid; k < Np; k += blockDim.x) {
+        const float y = k < nid ? phen[k] : -9.0f;
+        const bool ok = k < nid && (safe || y != -9.0f);
+        const double yc = s->y[k];
+        s->q[k] = ok ? (float)(yc * yc - c) : 0.0f;
+    }
+    for (int w = tid; w < Wp; w += blockDim.x) {
+        uint32_t bits = 0;
+        for (int t = 0; t < 32; ++t) {
+            const int k = 32 * w + t;
+            if (k < nid && (safe || phen[k] != -9.0f)) bits |= 1u << t;
+        }
+        s->wmask[w] = bits;
+    }
+}
+
+__global__ void k_finish(const Scratch *s, int64_t *nhits, float *maxf, int test_int)
+{
+    if (threadIdx.x != 0) return;
+    *nhits = (int64_t)s->counters[0];
+    if (maxf) {
+        maxf[0] = ord2f(s->maxf[0]);
+        maxf[1] = test_int ? ord2f(s->maxf[1]) : 0.0f;
+    }
+}
+
+constexpr int MAX_DEVICES = 64;
+static Scratch *g_addr[MAX_DEVICES];  // device address of g_scratch, per device (set-up)
+static int g_sms[MAX_DEVICES];
+
+}  // namespace noalloc
+}  // namespace epi
+
+extern "C" epi_status epi_scan_block_noalloc(const int32_t *d_gpack, int32_t nid, int32_t nsnp, const float *d_phen,
+                                             const epi_block *block, const epi_scan_opts *opts, epi_hit *d_hits,
+                                             int64_t cap, int64_t *d_nhits, float *d_maxf, void *stream)
+{
+    using namespace epi;
+    if (!d_gpack || !d_phen || !block || !opts || !d_nhits || cap < 0 || (cap > 0 && !d_hits) || nsnp < 1 || nid < 1)
+        return EPI_E_INVALID;
+    if (nid > EPI_NOALLOC_MAX_NID) return EPI_E_UNSUPPORTED;  // beyond the fixed scratch
+    if ((opts->test != 'f' && opts->test != 'i') || (opts->safe != 0 && opts->safe != 1)) return EPI_E_INVALID;
+    if (block->start1 < 0 || block->start2 < 0 || block->size1 < 0 || block->size2 < 0 ||
+        (int64_t)block->start1 + block->size1 > nsnp || (int64_t)block->start2 + block->size2 > nsnp)
+        return EPI_E_INVALID;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= noalloc::MAX_DEVICES) return EPI_E_NODEVICE;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t smem = sizeof(popc::Smem);
+
+    // once per device, with that device current: the scratch's device address
+    if (noalloc::g_addr[dev] == nullptr) {
+        int major = 0, sms = 0;
+        if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess || major != 10)
+            return EPI_E_NODEVICE;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return EPI_E_CUDA;
+        void *ptr = nullptr;
+        if (cudaGetSymbolAddress(&ptr, noalloc::g_scratch) != cudaSuccess || ptr == nullptr) return EPI_E_CUDA;
+        if (cudaFuncSetAttribute(popc::k_scan_popc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return EPI_E_CUDA;
+        noalloc::g_sms[dev] = sms;
+        noalloc::g_addr[dev] = (noalloc::Scratch *)ptr;
+    }
+    noalloc::Scratch *scr = noalloc::g_addr[dev];
+
+    const int Wp = ((nid + 31) / 32 + 3) / 4 * 4;
+    const int Np = 32 * Wp;
+    BlockDesc bd;
+    bd.start1 = block->start1;
+    bd.size1 = block->size1;
+    bd.start2 = block->start2;
+    bd.size2 = block->size2;
+    bd.tiles_i = (block->size1 + popc::TI - 1) / popc::TI;
+    bd.tiles_j = (block->size2 + popc::TJ - 1) / popc::TJ;
+    bd.tile_base = 0;
+    const long long ntiles = (long long)bd.tiles_i * bd.tiles_j;
+
+    ScanArgs a;
+    memset(&a, 0, sizeof(a));
+    a.gpack = d_gpack;
+    a.npack = nid / 16;
+    a.remain = nid % 16;
+    a.nid = nid;
+    a.nsnp = nsnp;
+    a.Wp = Wp;
+    a.Np = Np;
+    a.y = scr->y;
+    a.q = scr->q;
+    a.wmask = scr->wmask;
+    a.qc = &scr->qc;
+    a.ntraits = 1;
+    a.blocks = &scr->block;
+    a.nblocks = 1;
+    a.ntiles = ntiles;
+    a.test_int = opts->test == 'i';
+    a.safe = opts->safe;
+    a.report_trait = 0;
+    a.t1 = opts->t1;
+    a.t2 = opts->t2;
+    a.rows = reinterpret_cast<HitRow *>(d_hits);
+    a.cap = cap;
+    a.counters = scr->counters;
+    a.maxf = &scr->maxf[0];
+    a.maxf2 = &scr->maxf[1];
+
+    noalloc::k_prep<<<1, 1024, 0, st>>>(scr, d_phen, nid, Np, Wp, opts->safe, bd);
+    if (ntiles > 0) {
+        const int grid = (int)(ntiles < noalloc::g_sms[dev] ? ntiles : noalloc::g_sms[dev]);
+        popc::k_scan_popc<true><<<grid, popc::NT, smem, st>>>(a);
+    }
+    noalloc::k_finish<<<1, 32, 0, st>>>(scr, d_nhits, d_maxf, a.test_int);
+    if (cudaGetLastError() != cudaSuccess) return EPI_E_CUDA;
+    unsigned long long flags[2] = {0ull, 0ull};
+    if (cudaMemcpyAsync(flags, &scr->counters[2], sizeof(flags), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return EPI_E_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return EPI_E_CUDA;
+    return flags[0] ? EPI_E_TIMEOUT : EPI_OK;
+}

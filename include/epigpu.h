@@ -148,6 +148,39 @@ epi_status epi_last_timing(const epi_ctx *ctx, double *kernel_ms, int64_t *pairs
  * against the scan. */
 epi_status epi_get_stream(const epi_ctx *ctx, void **stream);
 
+/*
+ * Allocation-free scan of one block (no counterpart in the reference).
+ *
+ * For callers that cannot allocate GPU memory while they run: a service or real-time loop
+ * that forbids cudaMalloc after start-up, or a host framework that hands out device memory
+ * only from its own pool. Every input and output is a device buffer the caller owns; the
+ * call makes no cudaMalloc, cudaFree or other allocating call. The plain popcount form
+ * runs on the calling thread's current device, on `stream` (a cudaStream_t; NULL = the
+ * default stream), and the call returns once the scan has finished.
+ *
+ *   d_gpack  device, nsnp x (nid/16 + (nid%16 > 0)) int32: the reference's packed words
+ *   d_phen   device, nid floats; -9 = missing unless opts->safe
+ *   block    the pairs to scan (snp1 in block 1 > snp2 in block 2), as for epi_scan
+ *   opts     test, safe, t1, t2 as for epi_scan (form and chunk are ignored)
+ *   d_hits   device, cap rows: the hits, in no particular order (epi_scan gives the
+ *            reference's order; sort by (snp1, snp2) to compare)
+ *   d_nhits  device, one int64: the number of hits (may exceed cap; rows past cap are
+ *            dropped)
+ *   d_maxf   device, nullable, 2 floats: largest F and F2 over the block
+ *
+ * Working memory is a fixed array of about 520 KiB in this library, one per device, held
+ * until the process exits: it limits nid to EPI_NOALLOC_MAX_NID (larger returns
+ * EPI_E_UNSUPPORTED). The first call on each device looks up that array's device address;
+ * make that first call before any CUDA stream capture. All calls on a device share the
+ * array: calls that overlap on the GPU (other host threads, other streams) race and must
+ * be serialised by the caller.
+ */
+#define EPI_NOALLOC_MAX_NID 65535
+epi_status epi_scan_block_noalloc(const int32_t *d_gpack, int32_t nid, int32_t nsnp,
+                                  const float *d_phen, const epi_block *block,
+                                  const epi_scan_opts *opts, epi_hit *d_hits, int64_t cap,
+                                  int64_t *d_nhits, float *d_maxf, void *stream);
+
 /* The permutation of src/main.c:336-348 applied to a phenotype vector: srand(seed), then
  * glibc rand() Fisher-Yates from the end. Matches `epiGPU -A ... -p seed`. */
 void epi_permute_phenotype(float *phen, int32_t nid, uint32_t seed);
