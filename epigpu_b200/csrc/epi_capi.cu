@@ -22,6 +22,8 @@ namespace epi {
 cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int remain, uint4 *planes, int Wp,
                           uint32_t *codes, int Wc, uint8_t *hcodes, uint32_t *missbits, uint32_t *misssum, int Ws,
                           cudaStream_t stream);
+cudaError_t launch_misscount(const uint32_t *missbits, int nsnp, int Wp, int *cnt, cudaStream_t stream);
+cudaError_t launch_missfill(const uint32_t *missbits, int nsnp, int Wp, int stride, int *idx, cudaStream_t stream);
 cudaError_t launch_qmiss(const uint32_t *missbits, int nsnp, int Wp, const uint32_t *wmask, const double *qd, int Np,
                          int ntraits, double *qm, cudaStream_t stream);
 cudaError_t launch_popc(const ScanArgs &a, int grid, cudaStream_t stream);
@@ -32,6 +34,7 @@ bool mma_available();
 int mma_tile_i();
 int mma_tile_j();
 int mma_min_nid();
+int mma_max_nid();
 cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream);
 cudaError_t mma_encode_genotypes(MmaMaps *maps, const uint8_t *hcodes, int nsnp, int Np);
 cudaError_t mma_encode_traits(MmaMaps *maps, const int8_t *ydig, int ntraits, int Np);
@@ -54,7 +57,9 @@ struct epi_ctx {
     uint4 *d_planes = nullptr;
     uint8_t *d_hcodes = nullptr;
     uint32_t *d_missbits = nullptr, *d_misssum = nullptr;
-    size_t planes_cap = 0, hcodes_cap = 0, missbits_cap = 0, misssum_cap = 0;
+    int32_t *d_misscnt = nullptr, *d_missidx = nullptr;
+    int missstride = 0;
+    size_t planes_cap = 0, hcodes_cap = 0, missbits_cap = 0, misssum_cap = 0, misscnt_cap = 0, missidx_cap = 0;
     // traits
     int ntraits = 0, traits_nid = 0;
     float *d_y = nullptr, *d_q = nullptr;
@@ -179,7 +184,8 @@ epi_status epi_close(epi_ctx *ctx)
     if (!ctx) return EPI_OK;
     if (ctx->device >= 0) cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    void *bufs[] = {ctx->d_raw, ctx->d_planes, ctx->d_hcodes, ctx->d_missbits, ctx->d_misssum, ctx->d_y, ctx->d_q,
+    void *bufs[] = {ctx->d_raw, ctx->d_planes, ctx->d_hcodes, ctx->d_missbits, ctx->d_misssum, ctx->d_misscnt,
+                    ctx->d_missidx, ctx->d_y, ctx->d_q,
                     ctx->d_wmask, ctx->d_qc, ctx->d_yscale, ctx->d_qd, ctx->d_qtot, ctx->d_qm, ctx->d_ydig,
                     ctx->d_hits, ctx->d_counters, ctx->d_maxf, ctx->d_blocks};
     for (void *p : bufs)
@@ -222,7 +228,18 @@ epi_status epi_load_packed(epi_ctx *ctx, const int32_t *gpack, int32_t nid, int3
                        ctx->stream));
     CK(epi::launch_unpack(ctx->d_raw, nsnp, nid, npack, remain, ctx->d_planes, Wp, nullptr, Wc, ctx->d_hcodes,
                           ctx->d_missbits, ctx->d_misssum, Ws, ctx->stream));
+    // per-SNP lists of missing individuals (rows padded to the longest list)
+    CK(ensure(&ctx->d_misscnt, &ctx->misscnt_cap, (size_t)nsnp * sizeof(int32_t)));
+    CK(epi::launch_misscount(ctx->d_missbits, nsnp, Wp, ctx->d_misscnt, ctx->stream));
+    std::vector<int32_t> cnt((size_t)nsnp);
+    CK(cudaMemcpyAsync(cnt.data(), ctx->d_misscnt, (size_t)nsnp * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    const int stride = (std::max(1, *std::max_element(cnt.begin(), cnt.end())) + 3) / 4 * 4;  // 16-byte rows
+    CK(ensure(&ctx->d_missidx, &ctx->missidx_cap, (size_t)nsnp * stride * sizeof(int32_t)));
+    CK(epi::launch_missfill(ctx->d_missbits, nsnp, Wp, stride, ctx->d_missidx, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->missstride = stride;
     ctx->Ws = Ws;
     ctx->qm_valid = false;
     CK(epi::mma_encode_genotypes(&ctx->maps, ctx->d_hcodes, nsnp, 32 * Wp));
@@ -412,7 +429,8 @@ epi_status check_opts(epi_ctx *ctx, const epi_scan_opts *o)
 int pick_form(const epi_ctx *ctx, const epi_scan_opts *o)
 {
     if (o->form != EPI_FORM_AUTO) return o->form;
-    if (epi::mma_available() && ctx->nid >= epi::mma_min_nid()) return EPI_FORM_TENSOR;
+    if (epi::mma_available() && ctx->nid >= epi::mma_min_nid() && ctx->Np <= epi::mma_max_nid())
+        return EPI_FORM_TENSOR;
     return EPI_FORM_POPC;
 }
 
@@ -422,6 +440,8 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     r.form = pick_form(ctx, o);
     if (r.form == EPI_FORM_TENSOR && !epi::mma_available())
         return set_err(ctx, EPI_E_UNSUPPORTED, "tensor form not available in this build");
+    if (r.form == EPI_FORM_TENSOR && ctx->Np > epi::mma_max_nid())
+        return set_err(ctx, EPI_E_UNSUPPORTED, "tensor form: at most %d individuals", epi::mma_max_nid());
     if (r.form == EPI_FORM_POPC && ctx->nid > 65535)
         return set_err(ctx, EPI_E_UNSUPPORTED, "popcount form counts in 16 bits: at most 65535 individuals "
                        "(the reference's unsigned short counts, EpiOpenCL.c:68)");
@@ -469,6 +489,9 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     a.hcodes = ctx->d_hcodes;
     a.missbits = ctx->d_missbits;
     a.misssum = ctx->d_misssum;
+    a.missidx = ctx->d_missidx;
+    a.misscnt = ctx->d_misscnt;
+    a.missstride = ctx->missstride;
     a.Wp = ctx->Wp;
     a.Wc = ctx->Wc;
     a.Ws = ctx->Ws;

@@ -53,6 +53,8 @@ struct ScanArgs {
     const uint32_t *codes;
     const uint8_t *hcodes;
     const uint32_t *missbits, *misssum;
+    const int32_t *missidx, *misscnt;  // per SNP: missing individuals (row of missstride), count
+    int32_t missstride;
     int32_t Wp, Wc, Ws, nid, nsnp;
     // traits
     const float *y, *q;

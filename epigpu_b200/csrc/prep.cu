@@ -91,6 +91,44 @@ __global__ void k_qmiss(const uint32_t *__restrict__ missbits, int nsnp, int Wp,
     qm[gid] = x;
 }
 
+// Per SNP: number of individuals with a missing genotype.
+__global__ void k_misscount(const uint32_t *__restrict__ missbits, int nsnp, int Wp, int *__restrict__ cnt)
+{
+    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsnp) return;
+    int c = 0;
+    for (int w = 0; w < Wp; ++w) c += __popc(missbits[(size_t)s * Wp + w]);
+    cnt[s] = c;
+}
+
+// Per SNP: the indices of its missing individuals, ascending, in a row of `stride` entries.
+__global__ void k_missfill(const uint32_t *__restrict__ missbits, int nsnp, int Wp, int stride,
+                           int *__restrict__ idx)
+{
+    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsnp) return;
+    int n = 0;
+    for (int w = 0; w < Wp; ++w) {
+        uint32_t bits = missbits[(size_t)s * Wp + w];
+        while (bits) {
+            idx[(size_t)s * stride + n++] = 32 * w + __ffs(bits) - 1;
+            bits &= bits - 1;
+        }
+    }
+}
+
+cudaError_t launch_misscount(const uint32_t *missbits, int nsnp, int Wp, int *cnt, cudaStream_t stream)
+{
+    k_misscount<<<(nsnp + 255) / 256, 256, 0, stream>>>(missbits, nsnp, Wp, cnt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_missfill(const uint32_t *missbits, int nsnp, int Wp, int stride, int *idx, cudaStream_t stream)
+{
+    k_missfill<<<(nsnp + 255) / 256, 256, 0, stream>>>(missbits, nsnp, Wp, stride, idx);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int remain, uint4 *planes, int Wp,
                           uint32_t *codes, int Wc, uint8_t *hcodes, uint32_t *missbits, uint32_t *misssum, int Ws,
                           cudaStream_t stream)

@@ -57,6 +57,7 @@ constexpr uint32_t RAW_BYTES = (TI + TJ + 4) * KS;  // transaction bytes per raw
 constexpr int NWARPS = 14;
 constexpr int NTHREADS = NWARPS * 32;
 constexpr uint32_t IDESC = tc::idesc_i8(M, N);
+constexpr int MAX_NP = 32768;    // padded individuals: the epilogue bitmap takes 2 bytes each
 static_assert(RAW_J % 1024 == 0 && RAW_D >= RAW_J + TJ * KS && RAW_D + 4 * KS <= RAW_STAGE, "raw layout");
 
 struct Smem {
@@ -104,54 +105,76 @@ __device__ __forceinline__ uint32_t sel3(const uint32_t v[4], int idx)
     return idx == 0 ? v[0] : (idx == 1 ? v[1] : v[2]);
 }
 
-// sum over individuals missing on both SNPs (and phenotype-valid) of y^2
-__device__ __noinline__ double missing_both(const ScanArgs &a, int gi, int gj, int t)
+// 1/x for x > 0: single-precision seed (__frcp_rn) refined by one Newton step in FP64,
+// e = 1 - x r, r' = r + r e, which squares the seed's relative error (2^-24 -> ~2^-48).
+__device__ __forceinline__ double rcp_d(double x)
 {
-    double x = 0.0;
-    const uint32_t *si = a.misssum + (size_t)gi * a.Ws, *sj = a.misssum + (size_t)gj * a.Ws;
-    const uint32_t *mi = a.missbits + (size_t)gi * a.Wp, *mj = a.missbits + (size_t)gj * a.Wp;
-    const uint32_t *wt = a.wmask + (size_t)t * a.Wp;
-    const double *qt = a.qd + (size_t)t * a.Np;
-    for (int s = 0; s < a.Ws; ++s) {
-        uint32_t m = si[s] & sj[s];
-        while (m) {
-            const int w = 32 * s + __ffs(m) - 1;
-            m &= m - 1;
-            uint32_t bits = mi[w] & mj[w] & wt[w];
-            while (bits) {
-                x += qt[32 * w + __ffs(bits) - 1];
-                bits &= bits - 1;
-            }
-        }
-    }
-    return x;
+    double r = (double)__frcp_rn((float)x);
+    const double e = fma(-x, r, 1.0);
+    return fma(r, e, r);
 }
 
-struct PairIn {
-    int n[9];
-    long long s[9];
-};
-
-__device__ __noinline__ PairStat eval_pair(const ScanArgs &a, const PairIn in, int gi, int gj, int t, int di,
-                                           int dj, int size2)
+// The reference's 8 df / 4 df statistics (src/EpiOpenCL.c:231-247, :452-486) in FP64 from
+// the exact integer cell counts n and digit sums si (S = si * sc), and Q = sum of y^2 over
+// the pair's valid individuals. Same quantities as pair_stat, arranged to avoid division
+// chains: reciprocals of counts by rcp_d, one IEEE division for F and one for F2.
+__device__ __forceinline__ PairStat pair_stat_exact(const int n[9], const long long si[9], double sc, double Q,
+                                                    bool want_int)
 {
-    double S[9];
-    const double sc = a.yscale[t];
+    PairStat r;
+    int N = 0, nfac = 0;
+    long long St_i = 0;
 #pragma unroll
-    for (int c = 0; c < 9; ++c) S[c] = (double)in.s[c] * sc;
-    const double Q = a.qtot[t] - a.qm[(size_t)t * a.nsnp + gi] - a.qm[(size_t)t * a.nsnp + gj] +
-                     missing_both(a, gi, gj, t);
-    const PairStat s = pair_stat(in.n, S, Q, a.test_int != 0);
-    if (t == a.report_trait && (a.dump_counts || a.dump_F)) {
-        const size_t o = (size_t)di * size2 + dj;
-        if (a.dump_counts)
-            for (int c = 0; c < 9; ++c) a.dump_counts[9 * o + c] = in.n[c];
-        if (a.dump_F) a.dump_F[o] = (float)s.F;
-        if (a.dump_F2) a.dump_F2[o] = (float)s.F2;
-        if (a.dump_df1) a.dump_df1[o] = s.d1;
-        if (a.dump_df2) a.dump_df2[o] = s.d2;
+    for (int c = 0; c < 9; ++c) {
+        N += n[c];
+        St_i += si[c];
+        nfac += n[c] > 0;
     }
-    return s;
+    const double St = (double)St_i * sc;
+    const double m = St * rcp_d((double)N);
+    double mc[9], SSB = 0.0;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        mc[c] = 0.0;
+        if (n[c] > 0) {
+            mc[c] = (double)si[c] * sc * rcp_d((double)n[c]);
+            const double d = mc[c] - m;
+            SSB = fma((double)n[c] * d, d, SSB);
+        }
+    }
+    const double SSW = (Q - St * m) - SSB;
+    r.nfac = nfac;
+    r.d1 = nfac - 1;
+    r.d2 = N - nfac;
+    r.F = (SSB * (double)r.d2) / (SSW * (double)r.d1);
+    r.F2 = 0.0;
+    if (want_int) {
+        double row[3], col[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const long long rs = si[3 * i] + si[3 * i + 1] + si[3 * i + 2];
+            const long long cs = si[i] + si[i + 3] + si[i + 6];
+            const int rn = n[3 * i] + n[3 * i + 1] + n[3 * i + 2];
+            const int cn = n[i] + n[i + 3] + n[i + 6];
+            row[i] = rn > 0 ? (double)rs * sc * rcp_d((double)rn) : 0.0;
+            col[i] = cn > 0 ? (double)cs * sc * rcp_d((double)cn) : 0.0;
+        }
+        double SSI = 0.0;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            if (n[c] > 0) {
+                const double t = mc[c] - row[c / 3] - col[c % 3] + m;
+                SSI = fma((double)n[c] * t, t, SSI);
+            }
+        }
+        r.F2 = (SSI * (double)r.d2) / (4.0 * SSW);
+    }
+    return r;
+}
+
+__device__ __forceinline__ void named_sync(int id, int nthreads)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
 __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __grid_constant__ MmaMaps maps)
@@ -167,6 +190,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
     if (warp == 12) {
         tc::tmem_alloc(&sm.tmem_base, TMEM_COLS);
         tc::tmem_relinquish();
+    }
+    // per-CTA maxima of F and F2 per trait (flushed to global memory once, at the end)
+    unsigned int *smax = reinterpret_cast<unsigned int *>(reinterpret_cast<uint8_t *>(&sm) + sizeof(Smem) +
+                                                          (size_t)a.Np * 2);
+    {   // the epilogue's missing bitmap starts empty (it clears only the bits it sets)
+        uint32_t *bm = reinterpret_cast<uint32_t *>(reinterpret_cast<uint8_t *>(&sm) + sizeof(Smem));
+        for (int w = threadIdx.x; w < a.Np / 2; w += blockDim.x) bm[w] = 0u;
+        for (int w = threadIdx.x; w < 2 * a.ntraits; w += blockDim.x) smax[w] = 0u;
     }
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -190,6 +221,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
     tc::tc_fence_after();
     const uint32_t tmem = sm.tmem_base;
     volatile int *abort = &sm.abort;
+    // the tile's j-SNP missing bitmap: word k/2, bits 16*(k%2) + j' (j' < 16), one per individual
+    uint32_t *jbm = reinterpret_cast<uint32_t *>(reinterpret_cast<uint8_t *>(&sm) + sizeof(Smem));
 
     if (warp < 4) {
         // ---------------- A producers: TMEM lane = threadIdx.x ----------------
@@ -291,28 +324,89 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         }
     } else if (warp < 12) {
         // ---------------- epilogue ----------------
-        const int e = warp - 8;
+        const int e = warp - 8, et = threadIdx.x - 256;
         const int ii = 10 * e + lane / 3, ga = lane % 3, tbase = (lane / 3) * 3;
         const bool rowok = lane < 30;
         const uint32_t tl = tmem + ((uint32_t)(32 * e) << 16);
+        // bits j' of a 16-bit j mask that this lane evaluates (j' = 3 rho + ga)
+        const uint32_t mine = ga == 0 ? 0x9249u : (ga == 1 ? 0x2492u : 0x4924u);
         uint32_t accph[2] = {0u, 0u};
         int buf = 0;
         for (long long u = blockIdx.x; u < units; u += gridDim.x) {
             const Unit un = decode(a, u);
             if (un.skip) continue;
+            const int t = un.trait;
+            const double sc = a.yscale[t], qtot = a.qtot[t];
+            const int di = un.i0 + ii;
+            const bool ivalid = rowok && di < un.bd.size1;
+            const int gi = un.bd.start1 + (ivalid ? di : 0);
+            const double qmi = ivalid ? a.qm[(size_t)t * a.nsnp + gi] : 0.0;
+            // X: y^2 summed over individuals missing on both SNPs, through a bitmap of the
+            // tile's j-SNP missing individuals (set, read, cleared by the epilogue warps)
+            {
+                const int jj = et >> 3, part = et & 7;
+                if (un.j0 + jj < un.bd.size2) {
+                    const int gj = un.bd.start2 + un.j0 + jj, cnt = a.misscnt[gj];
+                    const int *L = a.missidx + (size_t)gj * a.missstride;
+                    for (int q = part; q < cnt; q += 8) {
+                        const int k = L[q];
+                        atomicOr(&jbm[k >> 1], (1u << jj) << (16 * (k & 1)));
+                    }
+                }
+            }
+            named_sync(1, 128);
+            double X[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            if (ivalid) {
+                const int cnt = a.misscnt[gi];
+                const int4 *L = reinterpret_cast<const int4 *>(a.missidx + (size_t)gi * a.missstride);
+                const double *qt = a.qd + (size_t)t * a.Np;
+#pragma unroll 4
+                for (int q = 0; q < (cnt + 3) / 4; ++q) {
+                    const int4 k4 = __ldg(L + q);
+                    const int ks[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+                    for (int e2 = 0; e2 < 4; ++e2) {
+                        if (4 * q + e2 >= cnt) break;
+                        const int k = ks[e2];
+                        uint32_t m = (jbm[k >> 1] >> (16 * (k & 1))) & mine;
+                        if (m) {
+                            const double wq = qt[k];
+                            while (m) {
+                                const int r = (__ffs(m) - 1) / 3;
+                                m &= m - 1;
+#pragma unroll
+                                for (int rr = 0; rr < 6; ++rr) X[rr] += (r == rr) ? wq : 0.0;
+                            }
+                        }
+                    }
+                }
+            }
+            named_sync(1, 128);
+            {
+                const int jj = et >> 3, part = et & 7;
+                if (un.j0 + jj < un.bd.size2) {
+                    const int gj = un.bd.start2 + un.j0 + jj, cnt = a.misscnt[gj];
+                    const int *L = a.missidx + (size_t)gj * a.missstride;
+                    for (int q = part; q < cnt; q += 8) jbm[L[q] >> 1] = 0u;
+                }
+            }
+            named_sync(1, 128);
+
             if (!tc::mbar_wait(&sm.acc_full[buf], accph[buf], abort)) {
                 fail(a, sm, 3);
                 break;
             }
             tc::tc_fence_after();
             const uint32_t acc = tl + (buf ? ACC_COL1 : 0);
-            const int t = un.trait;
             const bool report = a.report_trait < 0 || a.report_trait == t;
-            const int di = un.i0 + ii;
-            const bool ivalid = rowok && di < un.bd.size1;
 #pragma unroll 1
             for (int rho = 0; rho < (TJ + 2) / 3; ++rho) {
                 const int jb = 3 * rho;
+                const int dj = un.j0 + jb + ga;
+                const bool valid = ivalid && (jb + ga < TJ) && dj < un.bd.size2 &&
+                                   (un.bd.start1 + di > un.bd.start2 + dj);
+                const int gj = un.bd.start2 + (valid ? dj : 0);
+                const double qmj = valid ? a.qm[(size_t)t * a.nsnp + gj] : 0.0;
                 uint32_t v[NTYPE][4];
 #pragma unroll
                 for (int ty = 0; ty < NTYPE; ++ty) tc::tmem_ld4(acc + ty * TJ + jb, v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
@@ -324,40 +418,51 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     r1[ty] = __shfl_sync(0xffffffffu, sel3(v[ty], (ga + 2) % 3), tbase + (ga + 1) % 3);
                     r2[ty] = __shfl_sync(0xffffffffu, sel3(v[ty], (ga + 1) % 3), tbase + (ga + 2) % 3);
                 }
-                const int dj = un.j0 + jb + ga;
-                const bool valid = ivalid && (jb + ga < TJ) && dj < un.bd.size2 &&
-                                   (un.bd.start1 + di > un.bd.start2 + dj);
                 PairStat s;
                 s.nfac = s.d1 = s.d2 = 0;
                 s.F = s.F2 = 0.0;
                 if (valid) {
-                    PairIn in;
+                    // cells in row-major order, row a' = ga (own), ga+1 (r1), ga+2 (r2) mod 3
+                    int n[9];
+                    long long si[9];
 #pragma unroll
-                    for (int ap = 0; ap < 3; ++ap) {
-                        // row a' = ga + ap (mod 3): ap = 0 own, 1 from r1, 2 from r2
-                        const int arow = (ga + ap) % 3;
+                    for (int b = 0; b < 3; ++b) {
+                        const uint32_t w0[3] = {sel3(v[4 * b], ga), r1[4 * b], r2[4 * b]};
+                        const uint32_t w1[3] = {sel3(v[4 * b + 1], ga), r1[4 * b + 1], r2[4 * b + 1]};
+                        const uint32_t w2[3] = {sel3(v[4 * b + 2], ga), r1[4 * b + 2], r2[4 * b + 2]};
+                        const uint32_t w3[3] = {sel3(v[4 * b + 3], ga), r1[4 * b + 3], r2[4 * b + 3]};
 #pragma unroll
-                        for (int b = 0; b < 3; ++b) {
-                            uint32_t w0, w1, w2, w3;
-                            if (ap == 0) {
-                                w0 = sel3(v[4 * b], ga); w1 = sel3(v[4 * b + 1], ga);
-                                w2 = sel3(v[4 * b + 2], ga); w3 = sel3(v[4 * b + 3], ga);
-                            } else if (ap == 1) {
-                                w0 = r1[4 * b]; w1 = r1[4 * b + 1]; w2 = r1[4 * b + 2]; w3 = r1[4 * b + 3];
-                            } else {
-                                w0 = r2[4 * b]; w1 = r2[4 * b + 1]; w2 = r2[4 * b + 2]; w3 = r2[4 * b + 3];
-                            }
-                            const int cell = 3 * arow + b;
-                            in.n[cell] = (int)w0;
-                            in.s[cell] = (long long)(int)w1 + 256LL * (long long)(int)w2 + 65536LL * (long long)(int)w3;
+                        for (int ar = 0; ar < 3; ++ar) {
+                            // the source (0 own, 1 r1, 2 r2) holding genotype row ar
+                            const int src = (ar - ga + 3) % 3;
+                            const uint32_t c0 = src == 0 ? w0[0] : (src == 1 ? w0[1] : w0[2]);
+                            const uint32_t c1 = src == 0 ? w1[0] : (src == 1 ? w1[1] : w1[2]);
+                            const uint32_t c2 = src == 0 ? w2[0] : (src == 1 ? w2[1] : w2[2]);
+                            const uint32_t c3 = src == 0 ? w3[0] : (src == 1 ? w3[1] : w3[2]);
+                            n[3 * ar + b] = (int)c0;
+                            si[3 * ar + b] = (long long)(int)c1 + 256LL * (long long)(int)c2 +
+                                             65536LL * (long long)(int)c3;
                         }
                     }
-                    s = eval_pair(a, in, un.bd.start1 + di, un.bd.start2 + dj, t, di, dj, un.bd.size2);
+                    double xr = 0.0;
+#pragma unroll
+                    for (int rr = 0; rr < 6; ++rr) xr = (rr == rho) ? X[rr] : xr;
+                    s = pair_stat_exact(n, si, sc, qtot - qmi - qmj + xr, a.test_int != 0);
+                    if (t == a.report_trait && (a.dump_counts || a.dump_F)) {
+                        const size_t o = (size_t)di * un.bd.size2 + dj;
+                        if (a.dump_counts)
+#pragma unroll
+                            for (int c = 0; c < 9; ++c) a.dump_counts[9 * o + c] = n[c];
+                        if (a.dump_F) a.dump_F[o] = (float)s.F;
+                        if (a.dump_F2) a.dump_F2[o] = (float)s.F2;
+                        if (a.dump_df1) a.dump_df1[o] = s.d1;
+                        if (a.dump_df2) a.dump_df2[o] = s.d2;
+                    }
                 }
                 const bool hit = valid && report && is_hit(a, s);
                 emit_hit(a, hit, un.bd.start1 + di, un.bd.start2 + dj, s, t, un.block);
-                fold_max(&a.maxf[t], valid, s.F);
-                if (a.test_int) fold_max(&a.maxf2[t], valid, s.F2);
+                fold_max(&smax[t], valid, s.F);
+                if (a.test_int) fold_max(&smax[a.ntraits + t], valid, s.F2);
             }
             tc::tc_fence_before();
             __syncwarp();
@@ -452,6 +557,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         tc::tc_fence_after();
         tc::tmem_dealloc(tmem, TMEM_COLS);
     }
+    for (int w = threadIdx.x; w < 2 * a.ntraits; w += blockDim.x)
+        if (smax[w]) atomicMax(w < a.ntraits ? &a.maxf[w] : &a.maxf2[w - a.ntraits], smax[w]);
 }
 
 }  // namespace mma
@@ -495,12 +602,14 @@ bool mma_available() { return true; }
 int mma_tile_i() { return mma::TI; }
 int mma_tile_j() { return mma::TJ; }
 int mma_min_nid() { return 256; }
+int mma_max_nid() { return mma::MAX_NP; }
 int mma_stage_individuals() { return mma::KS; }
 
 cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream)
 {
-    // more than half of the SM's shared memory: one CTA per SM, which owns all 512 TMEM columns
-    const size_t smem = sizeof(mma::Smem) + 1024;
+    // more than half of the SM's shared memory: one CTA per SM, which owns all 512 TMEM columns;
+    // the tail holds the epilogue's missing bitmap, 2 bytes per individual
+    const size_t smem = sizeof(mma::Smem) + 1024 + (size_t)a.Np * 2 + 8 * (size_t)a.ntraits;
     static_assert(sizeof(mma::Smem) + 1024 > 116 * 1024, "one CTA per SM");
     cudaError_t e = cudaFuncSetAttribute(mma::k_scan_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

@@ -115,6 +115,9 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
     Smem &sm = *reinterpret_cast<Smem *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nstages = a.Wp / KW;
+    // per-CTA maxima of F and F2 per trait (flushed to global memory once, at the end)
+    unsigned int *smax = reinterpret_cast<unsigned int *>(smem_raw + sizeof(Smem));
+    for (int w = tid; w < 2 * a.ntraits; w += NT) smax[w] = 0u;
 
     for (;;) {
         if (tid == 0) sm.tile = (long long)atomicAdd(&a.counters[1], 1ull);
@@ -242,11 +245,14 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
                 const bool hit = valid && report && is_hit(a, s);
                 if (RAW) emit_row(a, hit, bd.start1 + gi, bd.start2 + gj, s);
                 else emit_hit(a, hit, bd.start1 + gi, bd.start2 + gj, s, t, b);
-                fold_max(&a.maxf[t], valid, s.F);
-                if (a.test_int) fold_max(&a.maxf2[t], valid, s.F2);
+                fold_max(&smax[t], valid, s.F);
+                if (a.test_int) fold_max(&smax[a.ntraits + t], valid, s.F2);
             }
         }
     }
+    __syncthreads();
+    for (int w = tid; w < 2 * a.ntraits; w += NT)
+        if (smax[w]) atomicMax(w < a.ntraits ? &a.maxf[w] : &a.maxf2[w - a.ntraits], smax[w]);
 }
 
 }  // namespace popc
@@ -258,7 +264,7 @@ int popc_words_multiple() { return popc::KW; }
 
 cudaError_t launch_popc(const ScanArgs &a, int grid, cudaStream_t stream)
 {
-    const size_t smem = sizeof(popc::Smem);
+    const size_t smem = sizeof(popc::Smem) + 8 * (size_t)a.ntraits;
     cudaError_t e =
         cudaFuncSetAttribute(popc::k_scan_popc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -401,7 +407,7 @@ extern "C" epi_status epi_scan_block_noalloc(const int32_t *d_gpack, int32_t nid
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= noalloc::MAX_DEVICES) return EPI_E_NODEVICE;
     cudaStream_t st = (cudaStream_t)stream;
-    const size_t smem = sizeof(popc::Smem);
+    const size_t smem = sizeof(popc::Smem) + 8;  // + per-CTA maxima of one trait
 
     // once per device, with that device current: the scratch's device address
     if (noalloc::g_addr[dev] == nullptr) {
