@@ -397,7 +397,9 @@ def main():
         pairs_launch = pairs_step
         if used_form == "tensor":
             int8 = int8_peak_tops()
-            ops_pair = 2.0 * 38.4 * nid  # int8 ops per pair (MMA shape 128x192 per 40x16 pairs)
+            # algorithmic int8 ops per pair: 3 genotype rows x 15 column types (3 x {count, 3 y
+            # digits} + 3 y^2 digits) per individual; the 128 x 240 tile carries 48 (padding rows)
+            ops_pair = 2.0 * 45.0 * nid
             achieved = pairs_launch * ops_pair / kern_s / 1e12
             roof = {"bound": "tensor", "achieved": achieved, "peak": int8, "unit": "TOP/s",
                     "frac": achieved / int8, "traffic": None,

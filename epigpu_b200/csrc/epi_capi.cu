@@ -20,12 +20,9 @@
 
 namespace epi {
 cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int remain, uint4 *planes, int Wp,
-                          uint32_t *codes, int Wc, uint8_t *hcodes, uint32_t *missbits, uint32_t *misssum, int Ws,
-                          cudaStream_t stream);
-cudaError_t launch_misscount(const uint32_t *missbits, int nsnp, int Wp, int *cnt, cudaStream_t stream);
-cudaError_t launch_missfill(const uint32_t *missbits, int nsnp, int Wp, int stride, int *idx, cudaStream_t stream);
-cudaError_t launch_qmiss(const uint32_t *missbits, int nsnp, int Wp, const uint32_t *wmask, const double *qd, int Np,
-                         int ntraits, double *qm, cudaStream_t stream);
+                          uint32_t *codes, int Wc, uint8_t *hcodes, uint32_t *missbits, cudaStream_t stream);
+cudaError_t launch_qmiss(const uint32_t *missbits, int nsnp, int Wp, const uint32_t *wmask, const double *qd,
+                        const double *qr, int Np, int ntraits, double *qm, double *rm, cudaStream_t stream);
 cudaError_t launch_popc(const ScanArgs &a, int grid, cudaStream_t stream);
 int popc_tile_i();
 int popc_tile_j();
@@ -51,15 +48,13 @@ struct epi_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // genotypes
     int nid = 0, nsnp = 0, npack = 0, remain = 0;
-    int Wp = 0, Wc = 0, Ws = 0, Np = 0;
+    int Wp = 0, Wc = 0, Np = 0;
     int32_t *d_raw = nullptr;
     size_t raw_cap = 0;
     uint4 *d_planes = nullptr;
     uint8_t *d_hcodes = nullptr;
-    uint32_t *d_missbits = nullptr, *d_misssum = nullptr;
-    int32_t *d_misscnt = nullptr, *d_missidx = nullptr;
-    int missstride = 0;
-    size_t planes_cap = 0, hcodes_cap = 0, missbits_cap = 0, misssum_cap = 0, misscnt_cap = 0, missidx_cap = 0;
+    uint32_t *d_missbits = nullptr;
+    size_t planes_cap = 0, hcodes_cap = 0, missbits_cap = 0;
     // traits
     int ntraits = 0, traits_nid = 0;
     float *d_y = nullptr, *d_q = nullptr;
@@ -184,8 +179,7 @@ epi_status epi_close(epi_ctx *ctx)
     if (!ctx) return EPI_OK;
     if (ctx->device >= 0) cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    void *bufs[] = {ctx->d_raw, ctx->d_planes, ctx->d_hcodes, ctx->d_missbits, ctx->d_misssum, ctx->d_misscnt,
-                    ctx->d_missidx, ctx->d_y, ctx->d_q,
+    void *bufs[] = {ctx->d_raw, ctx->d_planes, ctx->d_hcodes, ctx->d_missbits, ctx->d_y, ctx->d_q,
                     ctx->d_wmask, ctx->d_qc, ctx->d_yscale, ctx->d_qd, ctx->d_qtot, ctx->d_qm, ctx->d_ydig,
                     ctx->d_hits, ctx->d_counters, ctx->d_maxf, ctx->d_blocks};
     for (void *p : bufs)
@@ -218,29 +212,14 @@ epi_status epi_load_packed(epi_ctx *ctx, const int32_t *gpack, int32_t nid, int3
     const int npack1 = remain ? npack + 1 : npack;
     const int Wp = ((nid + 31) / 32 + 3) / 4 * 4;  // multiple of 4 words = 128 individuals
     const int Wc = 2 * Wp;
-    const int Ws = (Wp + 31) / 32;
     CK(ensure(&ctx->d_raw, &ctx->raw_cap, (size_t)nsnp * npack1 * sizeof(int32_t)));
     CK(ensure(&ctx->d_planes, &ctx->planes_cap, (size_t)nsnp * Wp * sizeof(uint4)));
     CK(ensure(&ctx->d_hcodes, &ctx->hcodes_cap, (size_t)nsnp * Wp * 32));
     CK(ensure(&ctx->d_missbits, &ctx->missbits_cap, (size_t)nsnp * Wp * sizeof(uint32_t)));
-    CK(ensure(&ctx->d_misssum, &ctx->misssum_cap, (size_t)nsnp * Ws * sizeof(uint32_t)));
     CK(cudaMemcpyAsync(ctx->d_raw, gpack, (size_t)nsnp * npack1 * sizeof(int32_t), cudaMemcpyHostToDevice,
                        ctx->stream));
     CK(epi::launch_unpack(ctx->d_raw, nsnp, nid, npack, remain, ctx->d_planes, Wp, nullptr, Wc, ctx->d_hcodes,
-                          ctx->d_missbits, ctx->d_misssum, Ws, ctx->stream));
-    // per-SNP lists of missing individuals (rows padded to the longest list)
-    CK(ensure(&ctx->d_misscnt, &ctx->misscnt_cap, (size_t)nsnp * sizeof(int32_t)));
-    CK(epi::launch_misscount(ctx->d_missbits, nsnp, Wp, ctx->d_misscnt, ctx->stream));
-    std::vector<int32_t> cnt((size_t)nsnp);
-    CK(cudaMemcpyAsync(cnt.data(), ctx->d_misscnt, (size_t)nsnp * sizeof(int32_t), cudaMemcpyDeviceToHost,
-                       ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    const int stride = (std::max(1, *std::max_element(cnt.begin(), cnt.end())) + 3) / 4 * 4;  // 16-byte rows
-    CK(ensure(&ctx->d_missidx, &ctx->missidx_cap, (size_t)nsnp * stride * sizeof(int32_t)));
-    CK(epi::launch_missfill(ctx->d_missbits, nsnp, Wp, stride, ctx->d_missidx, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    ctx->missstride = stride;
-    ctx->Ws = Ws;
+                          ctx->d_missbits, ctx->stream));
     ctx->qm_valid = false;
     CK(epi::mma_encode_genotypes(&ctx->maps, ctx->d_hcodes, nsnp, 32 * Wp));
     if (ctx->traits_nid != nid) ctx->ntraits = 0;  // traits no longer match
@@ -297,29 +276,35 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
             }
         }
     }
-    // tensor form: balanced base-256 digits of round(y * 2^sy) (|Y| <= 8355711 fits three
-    // int8 digits), the valid flag, and the quantised y^2
-    std::vector<int8_t> hd((size_t)ntraits * 4 * Np, 0);
-    std::vector<double> hqd((size_t)ntraits * Np, 0.0), hqtot(ntraits, 0.0), hsc(ntraits, 1.0);
+    // tensor form: per valid individual the flag, three balanced base-256 digits of
+    // Y = round(y * 2^sy) (|Y| <= 8355711), the quantised y^2 centred on the middle of its
+    // range, e = (Y 2^-sy)^2 - qcen, and three balanced digits of E = round(e / qstep)
+    // (|E| <= 8355711): the B columns that give the y^2 sum over individuals missing at the
+    // j-SNP. hqd holds e, then the residuals e - E qstep; hsc per trait 2^-sy, qcen, qstep.
+    constexpr int ND = 7;
+    std::vector<int8_t> hd((size_t)ntraits * ND * Np, 0);
+    std::vector<double> hqd(2 * (size_t)ntraits * Np, 0.0), hqtot(ntraits, 0.0), hsc(3 * (size_t)ntraits, 1.0);
     for (int t = 0; t < ntraits; ++t) {
         const float *yt = y + (size_t)t * nid;
+        auto ok = [&](int k) { return (hw[(size_t)t * Wp + k / 32] >> (k % 32) & 1u) != 0; };
         double sum = 0.0;
         long long nv = 0;
         for (int k = 0; k < nid; ++k)
-            if (hw[(size_t)t * Wp + k / 32] >> (k % 32) & 1u) {
+            if (ok(k)) {
                 sum += (double)yt[k];
                 ++nv;
             }
         const double mu = nv ? sum / (double)nv : 0.0;
         double maxabs = 0.0;
         for (int k = 0; k < nid; ++k)
-            if (hw[(size_t)t * Wp + k / 32] >> (k % 32) & 1u) maxabs = std::max(maxabs, std::fabs((double)yt[k] - mu));
+            if (ok(k)) maxabs = std::max(maxabs, std::fabs((double)yt[k] - mu));
         const int sy = (maxabs > 0.0 && std::isfinite(maxabs)) ? (int)std::floor(std::log2(8355000.0 / maxabs)) : 0;
         const double scale = std::ldexp(1.0, sy);
         hsc[t] = std::ldexp(1.0, -sy);
-        int8_t *d0 = hd.data() + (size_t)t * 4 * Np;
+        int8_t *d0 = hd.data() + (size_t)t * ND * Np;
+        double qmax = 0.0;
         for (int k = 0; k < nid; ++k) {
-            if (!(hw[(size_t)t * Wp + k / 32] >> (k % 32) & 1u)) continue;
+            if (!ok(k)) continue;
             long long Y = std::llround(((double)yt[k] - mu) * scale);
             Y = std::min(8355711LL, std::max(-8355711LL, Y));
             const long long a0 = ((Y + 128) & 255) - 128, Y1 = (Y - a0) / 256;
@@ -330,7 +315,24 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
             d0[3 * (size_t)Np + k] = (int8_t)a2;
             const double yq = (double)Y * hsc[t];
             hqd[(size_t)t * Np + k] = yq * yq;
-            hqtot[t] += yq * yq;
+            qmax = std::max(qmax, yq * yq);
+        }
+        const double qcen = 0.5 * qmax, qstep = qcen > 0.0 ? qcen / 8355711.0 : 1.0;
+        hsc[ntraits + t] = qcen;
+        hsc[2 * (size_t)ntraits + t] = qstep;
+        for (int k = 0; k < nid; ++k) {
+            if (!ok(k)) continue;
+            const double e = hqd[(size_t)t * Np + k] - qcen;
+            hqd[(size_t)t * Np + k] = e;
+            hqtot[t] += e;
+            long long E = std::llround(e / qstep);
+            E = std::min(8355711LL, std::max(-8355711LL, E));
+            const long long b0 = ((E + 128) & 255) - 128, E1 = (E - b0) / 256;
+            const long long b1 = ((E1 + 128) & 255) - 128, b2 = (E1 - b1) / 256;
+            d0[4 * (size_t)Np + k] = (int8_t)b0;
+            d0[5 * (size_t)Np + k] = (int8_t)b1;
+            d0[6 * (size_t)Np + k] = (int8_t)b2;
+            hqd[((size_t)ntraits + t) * Np + k] = e - (double)E * qstep;
         }
     }
     size_t need = (size_t)ntraits * Np * sizeof(float);
@@ -357,12 +359,12 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
     ctx->d_yscale = nullptr;
     size_t c1 = 0, c2 = 0;
     CK(ensure(&ctx->d_qtot, &c1, (size_t)ntraits * sizeof(double)));
-    CK(ensure(&ctx->d_yscale, &c2, (size_t)ntraits * sizeof(double)));
+    CK(ensure(&ctx->d_yscale, &c2, hsc.size() * sizeof(double)));
     CK(cudaMemcpyAsync(ctx->d_ydig, hd.data(), hd.size(), cudaMemcpyHostToDevice, ctx->stream));
     CK(epi::mma_encode_traits(&ctx->maps, ctx->d_ydig, ntraits, Np));
     CK(cudaMemcpyAsync(ctx->d_qd, hqd.data(), hqd.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->d_qtot, hqtot.data(), ntraits * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(ctx->d_yscale, hsc.data(), ntraits * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_yscale, hsc.data(), hsc.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->ntraits = ntraits;
     ctx->traits_nid = nid;
@@ -478,9 +480,11 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
         ctx->maxf_cap = 2 * ctx->ntraits;
     }
     if (r.form == EPI_FORM_TENSOR && !ctx->qm_valid) {
-        CK(ensure(&ctx->d_qm, &ctx->qm_cap, (size_t)ctx->ntraits * ctx->nsnp * sizeof(double)));
-        CK(epi::launch_qmiss(ctx->d_missbits, ctx->nsnp, ctx->Wp, ctx->d_wmask, ctx->d_qd, ctx->Np, ctx->ntraits,
-                             ctx->d_qm, ctx->stream));
+        const size_t tn = (size_t)ctx->ntraits * ctx->nsnp;
+        CK(ensure(&ctx->d_qm, &ctx->qm_cap, 2 * tn * sizeof(double)));
+        CK(epi::launch_qmiss(ctx->d_missbits, ctx->nsnp, ctx->Wp, ctx->d_wmask, ctx->d_qd,
+                             ctx->d_qd + (size_t)ctx->ntraits * ctx->Np, ctx->Np, ctx->ntraits, ctx->d_qm,
+                             ctx->d_qm + tn, ctx->stream));
         ctx->qm_valid = true;
     }
     epi::ScanArgs &a = r.args;
@@ -488,19 +492,17 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     a.planes = ctx->d_planes;
     a.hcodes = ctx->d_hcodes;
     a.missbits = ctx->d_missbits;
-    a.misssum = ctx->d_misssum;
-    a.missidx = ctx->d_missidx;
-    a.misscnt = ctx->d_misscnt;
-    a.missstride = ctx->missstride;
     a.Wp = ctx->Wp;
     a.Wc = ctx->Wc;
-    a.Ws = ctx->Ws;
     a.nid = ctx->nid;
     a.nsnp = ctx->nsnp;
     a.yscale = ctx->d_yscale;
+    a.qcen = ctx->d_yscale + ctx->ntraits;
+    a.qstep = ctx->d_yscale + 2 * (size_t)ctx->ntraits;
     a.qd = ctx->d_qd;
     a.qtot = ctx->d_qtot;
     a.qm = ctx->d_qm;
+    a.rm = ctx->d_qm + (size_t)ctx->ntraits * ctx->nsnp;
     a.ydig = ctx->d_ydig;
     a.y = ctx->d_y;
     a.q = ctx->d_q;

@@ -10,11 +10,14 @@
 //   wmask   uint32 [T][Wp]        phenotype-valid bits
 // and for the tensor-core form
 //   hcodes  uint8 [nsnp][Np]      one-hot genotype byte: 1 << g for g in 0..2, 0 if missing
-//   missbits uint32 [nsnp][Wp]    missing-genotype bits; misssum [nsnp][Ws] marks non-zero words
-//   ydig    int8 [T][4][Np]       per individual: phenotype-valid flag and the three balanced
-//                                 base-256 digits (low first) of round(y * 2^sy)
-//   qd      double [T][Np]        (quantised y)^2, 0 where invalid; qtot[T] its sum;
-//   qm      double [T][nsnp]      the part of qtot on individuals missing at that SNP
+//   missbits uint32 [nsnp][Wp]    missing-genotype bits
+//   ydig    int8 [T][7][Np]       per individual: phenotype-valid flag, the three balanced
+//                                 base-256 digits (low first) of round(y * 2^sy), and three
+//                                 of E = round(e / qstep) (e below)
+//   qd      double [2][T][Np]     e = (quantised y)^2 - qcen[t], then e - qstep[t] * E (the part
+//                                 the two digits do not hold), 0 where invalid; qtot[T] sum of e
+//   qm, rm  double [T][nsnp]      the sums of e and of the residuals over the individuals
+//                                 missing at that SNP
 // Individuals are padded to Np = 32*Wp (a multiple of 128); padding carries no genotype
 // and no phenotype.
 #pragma once
@@ -52,16 +55,15 @@ struct ScanArgs {
     const uint4 *planes;
     const uint32_t *codes;
     const uint8_t *hcodes;
-    const uint32_t *missbits, *misssum;
-    const int32_t *missidx, *misscnt;  // per SNP: missing individuals (row of missstride), count
-    int32_t missstride;
-    int32_t Wp, Wc, Ws, nid, nsnp;
+    const uint32_t *missbits;
+    int32_t Wp, Wc, nid, nsnp;
     // traits
     const float *y, *q;
     const uint32_t *wmask;
     const double *qc;          // [T]
     const double *yscale;      // [T] (tensor form: 2^-sy)
-    const double *qd, *qtot, *qm;
+    const double *qd, *qtot, *qm, *rm;
+    const double *qcen, *qstep;  // [T] (tensor form: centre and step of the 16-bit y^2 digits)
     const int8_t *ydig;
     int32_t Np, ntraits;
     // blocks / tiles

@@ -57,81 +57,32 @@ __global__ void k_unpack(const int32_t *__restrict__ raw, int nsnp, int nid, int
     }
 }
 
-// Per SNP: bit w' of summary word s marks a non-zero missing word 32 s + w'.
-__global__ void k_misssum(const uint32_t *__restrict__ missbits, int nsnp, int Wp, uint32_t *__restrict__ misssum,
-                          int Ws)
-{
-    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= (long long)nsnp * Ws) return;
-    const int s = (int)(gid / Ws), q = (int)(gid % Ws);
-    uint32_t m = 0;
-    for (int b = 0; b < 32; ++b) {
-        const int w = 32 * q + b;
-        if (w < Wp && missbits[(size_t)s * Wp + w] != 0u) m |= 1u << b;
-    }
-    misssum[gid] = m;
-}
-
-// qm[t][s] = sum over individuals missing at SNP s (and phenotype-valid for t) of qd[t][k]
+// Per trait t and SNP s, over the individuals missing at s (and phenotype-valid for t):
+// qm[t][s] = sum of qd[t][k] and, when qr is given, rm[t][s] = sum of qr[t][k]
 __global__ void k_qmiss(const uint32_t *__restrict__ missbits, int nsnp, int Wp, const uint32_t *__restrict__ wmask,
-                        const double *__restrict__ qd, int Np, int ntraits, double *__restrict__ qm)
+                        const double *__restrict__ qd, const double *__restrict__ qr, int Np, int ntraits,
+                        double *__restrict__ qm, double *__restrict__ rm)
 {
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= (long long)nsnp * ntraits) return;
     const int t = (int)(gid / nsnp), s = (int)(gid % nsnp);
-    double x = 0.0;
+    double x = 0.0, r = 0.0;
     const uint32_t *mb = missbits + (size_t)s * Wp;
     for (int w = 0; w < Wp; ++w) {
         uint32_t bits = mb[w] & wmask[(size_t)t * Wp + w];
         while (bits) {
-            x += qd[(size_t)t * Np + 32 * w + __ffs(bits) - 1];
+            const size_t k = (size_t)t * Np + 32 * w + __ffs(bits) - 1;
+            x += qd[k];
+            if (qr) r += qr[k];
             bits &= bits - 1;
         }
     }
     qm[gid] = x;
-}
-
-// Per SNP: number of individuals with a missing genotype.
-__global__ void k_misscount(const uint32_t *__restrict__ missbits, int nsnp, int Wp, int *__restrict__ cnt)
-{
-    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nsnp) return;
-    int c = 0;
-    for (int w = 0; w < Wp; ++w) c += __popc(missbits[(size_t)s * Wp + w]);
-    cnt[s] = c;
-}
-
-// Per SNP: the indices of its missing individuals, ascending, in a row of `stride` entries.
-__global__ void k_missfill(const uint32_t *__restrict__ missbits, int nsnp, int Wp, int stride,
-                           int *__restrict__ idx)
-{
-    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nsnp) return;
-    int n = 0;
-    for (int w = 0; w < Wp; ++w) {
-        uint32_t bits = missbits[(size_t)s * Wp + w];
-        while (bits) {
-            idx[(size_t)s * stride + n++] = 32 * w + __ffs(bits) - 1;
-            bits &= bits - 1;
-        }
-    }
-}
-
-cudaError_t launch_misscount(const uint32_t *missbits, int nsnp, int Wp, int *cnt, cudaStream_t stream)
-{
-    k_misscount<<<(nsnp + 255) / 256, 256, 0, stream>>>(missbits, nsnp, Wp, cnt);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_missfill(const uint32_t *missbits, int nsnp, int Wp, int stride, int *idx, cudaStream_t stream)
-{
-    k_missfill<<<(nsnp + 255) / 256, 256, 0, stream>>>(missbits, nsnp, Wp, stride, idx);
-    return cudaGetLastError();
+    if (rm) rm[gid] = r;
 }
 
 cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int remain, uint4 *planes, int Wp,
-                          uint32_t *codes, int Wc, uint8_t *hcodes, uint32_t *missbits, uint32_t *misssum, int Ws,
-                          cudaStream_t stream)
+                          uint32_t *codes, int Wc, uint8_t *hcodes, uint32_t *missbits, cudaStream_t stream)
 {
     const int npack1 = remain ? npack + 1 : npack;
     const long long total = (long long)nsnp * Wp;
@@ -139,19 +90,16 @@ cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int 
     const long long nb = (total + nt - 1) / nt;
     k_unpack<<<(unsigned)nb, nt, 0, stream>>>(raw, nsnp, nid, npack, remain, npack1, planes, Wp, codes, Wc, hcodes,
                                               missbits);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess || misssum == nullptr) return e;
-    const long long t2 = (long long)nsnp * Ws;
-    k_misssum<<<(unsigned)((t2 + nt - 1) / nt), nt, 0, stream>>>(missbits, nsnp, Wp, misssum, Ws);
     return cudaGetLastError();
 }
 
-cudaError_t launch_qmiss(const uint32_t *missbits, int nsnp, int Wp, const uint32_t *wmask, const double *qd, int Np,
-                         int ntraits, double *qm, cudaStream_t stream)
+cudaError_t launch_qmiss(const uint32_t *missbits, int nsnp, int Wp, const uint32_t *wmask, const double *qd,
+                        const double *qr, int Np, int ntraits, double *qm, double *rm, cudaStream_t stream)
 {
     const long long total = (long long)nsnp * ntraits;
     const int nt = 256;
-    k_qmiss<<<(unsigned)((total + nt - 1) / nt), nt, 0, stream>>>(missbits, nsnp, Wp, wmask, qd, Np, ntraits, qm);
+    k_qmiss<<<(unsigned)((total + nt - 1) / nt), nt, 0, stream>>>(missbits, nsnp, Wp, wmask, qd, qr, Np, ntraits, qm,
+                                                                     rm);
     return cudaGetLastError();
 }
 

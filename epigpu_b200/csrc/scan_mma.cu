@@ -4,32 +4,46 @@
 // counts and phenotype sums (src/EpiOpenCL.c:110-228). Both are contractions over k:
 //     n_ab = sum_k [g_i(k)=a] [g_j(k)=b] w_k        S_ab = sum_k [g_i(k)=a] [g_j(k)=b] y_k
 // so for a tile of 40 i-SNPs x 16 j-SNPs they are one integer GEMM
-//     D[128 x 192] = A[128 x K] * B[K x 192]
+//     D[128 x 240] = A[128 x K] * B[K x 240]
 //   A rows (TMEM lane 32w + l, l < 30): i-SNP 10w + l/3, genotype a = l%3: [g_i(k) == a]
-//   B cols (type t = 4b + s, column 16t + j'): [g_j(k) == b] * D_s(k) with D_0 = w_k
-//     (phenotype valid) and D_1..3 the balanced base-256 digits of the fixed-point
-//     phenotype Y_k = round(y_k * 2^sy) (y centred, 0 when invalid).
+//   B cols (type t, column 16t + j'):
+//     t = 4b + s (t < 12): [g_j(k) == b] * D_s(k), D_0 = w_k (phenotype valid) and D_1..3 the
+//       balanced base-256 digits of the fixed-point phenotype Y_k = round(y_k * 2^sy)
+//       (y centred, 0 when invalid);
+//     t = 12..14: [g_j(k) missing] * E_s(k), the three balanced digits of
+//       E_k = round((ytilde_k^2 - qcen) / qstep), ytilde = Y 2^-sy (0 when invalid).
+// issued as two MMAs per K step: columns 0-191 into a double-buffered accumulator, columns
+// 192-239 (the E sums) into a single one that the epilogue copies to shared memory first.
 // int8 operands, int32 accumulation: counts and digit sums are exact, so
 //     S_ab = (D1 + 256 D2 + 65536 D3) * 2^-sy exactly for the quantised phenotype.
-// The sum of y^2 over the pair's valid individuals comes from per-SNP FP64 terms and the
-// (sparse) individuals missing on both SNPs:  Q_ij = Qtot - QM_i - QM_j + X_ij.
-// The epilogue forms SSB / SSI / F / F2 in FP64 (pair_stat) from these exact inputs.
+// The sum of ytilde^2 over the pair's valid individuals (both genotypes known, phenotype
+// valid) is, with e_k = ytilde_k^2 - qcen = qstep E_k + r_k,
+//     Q_ij = qcen * N_ij + (qtot - QM_i) - sum_k [g_i(k) known] [g_j(k) missing] e_k
+// where qtot - QM_i = sum of e over individuals known at i (exact FP64, per SNP), and the
+// last sum is qstep times the t = 12, 13 columns summed over a, plus the residuals r over the
+// same individuals, taken as RM_j (r summed over all individuals missing at j, FP64, per
+// SNP). The one approximation: the residuals of individuals missing at both SNPs are counted
+// in RM_j, an error of at most qstep / 2 per such individual (qstep = max(ytilde^2) / 2^24).
+// The epilogue forms SSB / SSI / F / F2 in FP64.
 //
 // Persistent kernel, one CTA per SM, warp-specialised, 14 warps:
 //   warp 13     TMA loader (one thread): per 128-individual stage, three 2-D tiled loads
 //               (no multicast) into a 6-deep raw ring: the i-tile's and j-tile's one-hot
-//               genotype bytes (40 and 16 rows x 128 B) and the trait's 4 digit rows, all
+//               genotype bytes (40 and 16 rows x 128 B) and the trait's 6 digit rows,
 //               128-byte swizzled; completion by mbarrier transaction bytes
 //   warps 0-3   A producers: one TMEM lane each; expand the raw i rows into the stage's A
 //               rows and store them into TMEM with tcgen05.st (the MMA reads A from TMEM)
 //   warps 4-7   B producers: expand raw j rows x digits into the stage's B tile (K-major,
 //               128-byte swizzle) in smem
-//   warps 8-11  epilogue: tcgen05.ld of the accumulator, lane-triplet shuffles, FP64
-//               statistics, warp-aggregated hit append, per-trait max F
-//   warp 12     TMEM allocator and MMA issuer (one thread): 4 x tcgen05.mma per stage
-// 4-stage operand pipeline, 2 TMEM accumulators (columns 0 and 192) so the epilogue of one
-// tile overlaps the MMAs of the next. All waits are bounded (tc_ptx.cuh); a timeout sets
-// counters[2] and every role leaves its loop.
+//   warps 8-11  epilogue: copy of the E accumulator to shared memory, tcgen05.ld of the
+//               main accumulator, lane-triplet shuffles, FP64 statistics, warp-aggregated
+//               hit append, per-trait max F
+//   warp 12     TMEM allocator and MMA issuer (one thread): 8 x tcgen05.mma per stage
+// TMEM (512 columns): accumulators 0 and 1 at [0, 192) and [192, 384), the E accumulator at
+// [384, 432), A stages at [432, 464) and [464, 496). 4-stage B ring, 2-stage A ring, 2 main
+// accumulators, so the epilogue of one tile overlaps the MMAs of the next (which wait only for
+// the short E copy). All waits are bounded (tc_ptx.cuh); a timeout sets counters[2] and every
+// role leaves its loop.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -41,29 +55,42 @@ namespace mma {
 
 constexpr int TI = 40;         // i-SNPs per tile (4 warps x 10 lane triplets)
 constexpr int TJ = 16;         // j-SNPs per tile
-constexpr int NTYPE = 12;      // B column types per j-SNP: b (3) x {w, digit0, digit1, digit2}
-constexpr int N = TJ * NTYPE;  // 192
+constexpr int NTY = 12;        // main B column types per j-SNP: b (3) x {w, d0, d1, d2}
+constexpr int NE = 3;          // E column types per j-SNP: missing x {e0, e1, e2}
+constexpr int N1 = TJ * NTY;   // 192
+constexpr int N2 = TJ * NE;    // 48
+constexpr int NB = N1 + N2;    // B tile rows (240)
 constexpr int M = 128;
 constexpr int KS = 128;        // individuals per pipeline stage
-constexpr int STAGES = 4;
-constexpr int ACC_COL1 = 192;  // second accumulator; first at column 0
-constexpr int A_COL = 384;     // A stage s at TMEM columns A_COL + 32 s
+constexpr int STAGES = 4;      // B ring (smem)
+constexpr int ASTAGES = 2;     // A ring (TMEM)
+constexpr int ND = 7;          // digit rows per trait: w, Y digits (3), E digits (3)
+constexpr uint32_t ACC_COL0 = 0, ACC_COL1 = 192, ACC_E = 384, A_COL0 = 432, A_COL1 = 464;
+constexpr int ESTRIDE = 52;    // words per lane row of the E copy in smem (48 used)
+__host__ __device__ constexpr uint32_t acc_col(uint32_t buf) { return buf ? ACC_COL1 : ACC_COL0; }
+__host__ __device__ constexpr uint32_t a_col(uint32_t s) { return s ? A_COL1 : A_COL0; }
 constexpr uint32_t TMEM_COLS = 512;
-constexpr int B_STAGE = N * KS;  // bytes per B stage (24 KB)
+constexpr int B_STAGE = NB * KS;  // bytes per B stage (30 KB)
 constexpr int RSTAGES = 6;       // raw (TMA) ring depth
-constexpr int RAW_I = 0, RAW_J = TI * KS, RAW_D = RAW_I + 7 * 1024;  // 1024-aligned offsets in a raw stage
-constexpr int RAW_STAGE = 8192;
-constexpr uint32_t RAW_BYTES = (TI + TJ + 4) * KS;  // transaction bytes per raw stage
+// raw stage: one-hot genotype rows (40 i, 16 j) and the trait's digit rows
+constexpr int RAW_I = 0, RAW_J = TI * KS, RAW_D = RAW_J + TJ * KS;
+constexpr int RAW_STAGE = 8 * 1024;
+constexpr uint32_t RAW_BYTES = (TI + TJ + ND) * KS;  // transaction bytes per raw stage
 constexpr int NWARPS = 14;
 constexpr int NTHREADS = NWARPS * 32;
-constexpr uint32_t IDESC = tc::idesc_i8(M, N);
-constexpr int MAX_NP = 32768;    // padded individuals: the epilogue bitmap takes 2 bytes each
-static_assert(RAW_J % 1024 == 0 && RAW_D >= RAW_J + TJ * KS && RAW_D + 4 * KS <= RAW_STAGE, "raw layout");
+constexpr uint32_t IDESC1 = tc::idesc_i8(M, N1), IDESC2 = tc::idesc_i8(M, N2);
+static_assert(RAW_J % 1024 == 0 && RAW_D % 1024 == 0 && RAW_D + ND * KS <= RAW_STAGE, "raw layout");
+static_assert(B_STAGE % 1024 == 0 && (N1 * KS) % 1024 == 0 && N1 % 16 == 0 && N2 % 16 == 0, "B tile");
+static_assert(ASTAGES == 2 && ACC_COL0 + N1 <= ACC_COL1 && ACC_COL1 + N1 <= ACC_E && ACC_E + N2 <= A_COL0 &&
+                  A_COL0 + KS / 4 <= A_COL1 && A_COL1 + KS / 4 <= TMEM_COLS,
+              "TMEM layout");
 
 struct Smem {
     uint8_t b[STAGES][B_STAGE];
     uint8_t raw[RSTAGES][RAW_STAGE];
-    uint64_t full[STAGES], empty[STAGES], raw_full[RSTAGES], raw_empty[RSTAGES], acc_full[2], acc_empty[2], drain;
+    int32_t esum[4 * 32][ESTRIDE];  // per TMEM lane: the tile's E accumulator row
+    uint64_t full[STAGES], empty[STAGES], afull[ASTAGES], aempty[ASTAGES], raw_full[RSTAGES], raw_empty[RSTAGES],
+        acc_full[2], acc_empty[2], e_empty, drain;
     uint32_t tmem_base;
     int abort;
 };
@@ -172,9 +199,13 @@ __device__ __forceinline__ PairStat pair_stat_exact(const int n[9], const long l
     return r;
 }
 
-__device__ __forceinline__ void named_sync(int id, int nthreads)
+template <int RING>
+__device__ __forceinline__ void advance(uint32_t &slot, uint32_t &phase)
 {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+    if (++slot == RING) {
+        slot = 0;
+        phase ^= 1u;
+    }
 }
 
 __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __grid_constant__ MmaMaps maps)
@@ -192,17 +223,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         tc::tmem_relinquish();
     }
     // per-CTA maxima of F and F2 per trait (flushed to global memory once, at the end)
-    unsigned int *smax = reinterpret_cast<unsigned int *>(reinterpret_cast<uint8_t *>(&sm) + sizeof(Smem) +
-                                                          (size_t)a.Np * 2);
-    {   // the epilogue's missing bitmap starts empty (it clears only the bits it sets)
-        uint32_t *bm = reinterpret_cast<uint32_t *>(reinterpret_cast<uint8_t *>(&sm) + sizeof(Smem));
-        for (int w = threadIdx.x; w < a.Np / 2; w += blockDim.x) bm[w] = 0u;
-        for (int w = threadIdx.x; w < 2 * a.ntraits; w += blockDim.x) smax[w] = 0u;
-    }
+    unsigned int *smax = reinterpret_cast<unsigned int *>(reinterpret_cast<uint8_t *>(&sm) + sizeof(Smem));
+    for (int w = threadIdx.x; w < 2 * a.ntraits; w += blockDim.x) smax[w] = 0u;
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
-            tc::mbar_init(&sm.full[s], 8);
+            tc::mbar_init(&sm.full[s], 4);
             tc::mbar_init(&sm.empty[s], 1);
+        }
+        for (int s = 0; s < ASTAGES; ++s) {
+            tc::mbar_init(&sm.afull[s], 4);
+            tc::mbar_init(&sm.aempty[s], 1);
         }
         for (int r = 0; r < RSTAGES; ++r) {
             tc::mbar_init(&sm.raw_full[r], 1);
@@ -212,6 +242,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             tc::mbar_init(&sm.acc_full[b], 1);
             tc::mbar_init(&sm.acc_empty[b], 4);
         }
+        tc::mbar_init(&sm.e_empty, 4);
         tc::mbar_init(&sm.drain, 1);
         sm.abort = 0;
         tc::fence_barrier_init();
@@ -221,21 +252,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
     tc::tc_fence_after();
     const uint32_t tmem = sm.tmem_base;
     volatile int *abort = &sm.abort;
-    // the tile's j-SNP missing bitmap: word k/2, bits 16*(k%2) + j' (j' < 16), one per individual
-    uint32_t *jbm = reinterpret_cast<uint32_t *>(reinterpret_cast<uint8_t *>(&sm) + sizeof(Smem));
 
     if (warp < 4) {
         // ---------------- A producers: TMEM lane = threadIdx.x ----------------
         const int ii = 10 * warp + lane / 3, ga = lane % 3;
         const bool rowok = lane < 30;
-        const uint32_t taddr_lane = tmem + ((uint32_t)(32 * warp) << 16) + A_COL;
-        uint32_t stage = 0, phase = 0, rs = 0, rph = 0;
+        const uint32_t taddr_lane = tmem + ((uint32_t)(32 * warp) << 16);
+        uint32_t as = 0, aph = 0, rs = 0, rph = 0;
         bool ok = true;
         for (long long u = blockIdx.x; u < units && ok; u += gridDim.x) {
             const Unit un = decode(a, u);
             if (un.skip) continue;
             for (int ks = 0; ks < nks; ++ks) {
-                if (!tc::mbar_wait(&sm.raw_full[rs], rph, abort) || !tc::mbar_wait(&sm.empty[stage], phase ^ 1u, abort)) {
+                if (!tc::mbar_wait(&sm.raw_full[rs], rph, abort) || !tc::mbar_wait(&sm.aempty[as], aph ^ 1u, abort)) {
                     fail(a, sm, 1);
                     ok = false;
                     break;
@@ -250,22 +279,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     v[4 * c + 2] = (h.z >> ga) & 0x01010101u;
                     v[4 * c + 3] = (h.w >> ga) & 0x01010101u;
                 }
-                tc::tmem_st32(taddr_lane + 32 * stage, v);
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&sm.raw_empty[rs]);
+                tc::tmem_st32(taddr_lane + a_col(as), v);
                 tc::tmem_wait_st();
                 tc::tc_fence_before();
                 __syncwarp();
-                if (lane == 0) {
-                    tc::mbar_arrive(&sm.full[stage]);
-                    tc::mbar_arrive(&sm.raw_empty[rs]);
-                }
-                if (++stage == STAGES) {
-                    stage = 0;
-                    phase ^= 1u;
-                }
-                if (++rs == RSTAGES) {
-                    rs = 0;
-                    rph ^= 1u;
-                }
+                if (lane == 0) tc::mbar_arrive(&sm.afull[as]);
+                advance<ASTAGES>(as, aph);
+                advance<RSTAGES>(rs, rph);
             }
         }
     } else if (warp < 8) {
@@ -284,10 +306,21 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 }
                 const uint8_t *raw = sm.raw[rs];
                 const uint4 h = ld_sw128(raw + RAW_J, jj, c);
-                uint4 d[4];
+                uint4 d[ND];
 #pragma unroll
-                for (int s2 = 0; s2 < 4; ++s2) d[s2] = ld_sw128(raw + RAW_D, s2, c);
+                for (int s2 = 0; s2 < ND; ++s2) d[s2] = ld_sw128(raw + RAW_D, s2, c);
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&sm.raw_empty[rs]);
                 uint8_t *base = sm.b[stage];
+                auto put = [&](int ty, const uint4 &m, const uint4 &dv) {
+                    const int n = ty * TJ + jj;
+                    uint4 o;
+                    o.x = m.x & dv.x;
+                    o.y = m.y & dv.y;
+                    o.z = m.z & dv.z;
+                    o.w = m.w & dv.w;
+                    *reinterpret_cast<uint4 *>(base + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4)) = o;
+                };
 #pragma unroll
                 for (int b = 0; b < 3; ++b) {
                     uint4 m;
@@ -296,125 +329,83 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     m.z = ((h.z >> b) & 0x01010101u) * 0xFFu;
                     m.w = ((h.w >> b) & 0x01010101u) * 0xFFu;
 #pragma unroll
-                    for (int s2 = 0; s2 < 4; ++s2) {
-                        const int n = (4 * b + s2) * TJ + jj;
-                        uint4 o;
-                        o.x = m.x & d[s2].x;
-                        o.y = m.y & d[s2].y;
-                        o.z = m.z & d[s2].z;
-                        o.w = m.w & d[s2].w;
-                        *reinterpret_cast<uint4 *>(base + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4)) = o;
-                    }
+                    for (int s2 = 0; s2 < 4; ++s2) put(4 * b + s2, m, d[s2]);
                 }
+                // missing genotype: one-hot byte 0 (bits 0-2 clear); the shifts only move
+                // bits of the next byte into bits 6-7 of this one, which the mask drops
+                uint4 mm;
+                mm.x = (((h.x | (h.x >> 1) | (h.x >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
+                mm.y = (((h.y | (h.y >> 1) | (h.y >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
+                mm.z = (((h.z | (h.z >> 1) | (h.z >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
+                mm.w = (((h.w | (h.w >> 1) | (h.w >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
+                put(12, mm, d[4]);
+                put(13, mm, d[5]);
+                put(14, mm, d[6]);
                 tc::fence_proxy_async_smem();
                 __syncwarp();
-                if (lane == 0) {
-                    tc::mbar_arrive(&sm.full[stage]);
-                    tc::mbar_arrive(&sm.raw_empty[rs]);
-                }
-                if (++stage == STAGES) {
-                    stage = 0;
-                    phase ^= 1u;
-                }
-                if (++rs == RSTAGES) {
-                    rs = 0;
-                    rph ^= 1u;
-                }
+                if (lane == 0) tc::mbar_arrive(&sm.full[stage]);
+                advance<STAGES>(stage, phase);
+                advance<RSTAGES>(rs, rph);
             }
         }
     } else if (warp < 12) {
         // ---------------- epilogue ----------------
-        const int e = warp - 8, et = threadIdx.x - 256;
+        const int e = warp - 8;
         const int ii = 10 * e + lane / 3, ga = lane % 3, tbase = (lane / 3) * 3;
         const bool rowok = lane < 30;
         const uint32_t tl = tmem + ((uint32_t)(32 * e) << 16);
-        // bits j' of a 16-bit j mask that this lane evaluates (j' = 3 rho + ga)
-        const uint32_t mine = ga == 0 ? 0x9249u : (ga == 1 ? 0x2492u : 0x4924u);
+        int32_t(*esum)[ESTRIDE] = sm.esum + 32 * e;  // this warp's 32 lane rows
         uint32_t accph[2] = {0u, 0u};
         int buf = 0;
         for (long long u = blockIdx.x; u < units; u += gridDim.x) {
             const Unit un = decode(a, u);
             if (un.skip) continue;
             const int t = un.trait;
-            const double sc = a.yscale[t], qtot = a.qtot[t];
+            const double sc = a.yscale[t], qcen = a.qcen[t], qstep = a.qstep[t];
             const int di = un.i0 + ii;
             const bool ivalid = rowok && di < un.bd.size1;
             const int gi = un.bd.start1 + (ivalid ? di : 0);
-            const double qmi = ivalid ? a.qm[(size_t)t * a.nsnp + gi] : 0.0;
-            // X: y^2 summed over individuals missing on both SNPs, through a bitmap of the
-            // tile's j-SNP missing individuals (set, read, cleared by the epilogue warps)
-            {
-                const int jj = et >> 3, part = et & 7;
-                if (un.j0 + jj < un.bd.size2) {
-                    const int gj = un.bd.start2 + un.j0 + jj, cnt = a.misscnt[gj];
-                    const int *L = a.missidx + (size_t)gj * a.missstride;
-                    for (int q = part; q < cnt; q += 8) {
-                        const int k = L[q];
-                        atomicOr(&jbm[k >> 1], (1u << jj) << (16 * (k & 1)));
-                    }
-                }
-            }
-            named_sync(1, 128);
-            double X[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-            if (ivalid) {
-                const int cnt = a.misscnt[gi];
-                const int4 *L = reinterpret_cast<const int4 *>(a.missidx + (size_t)gi * a.missstride);
-                const double *qt = a.qd + (size_t)t * a.Np;
-#pragma unroll 4
-                for (int q = 0; q < (cnt + 3) / 4; ++q) {
-                    const int4 k4 = __ldg(L + q);
-                    const int ks[4] = {k4.x, k4.y, k4.z, k4.w};
-#pragma unroll
-                    for (int e2 = 0; e2 < 4; ++e2) {
-                        if (4 * q + e2 >= cnt) break;
-                        const int k = ks[e2];
-                        uint32_t m = (jbm[k >> 1] >> (16 * (k & 1))) & mine;
-                        if (m) {
-                            const double wq = qt[k];
-                            while (m) {
-                                const int r = (__ffs(m) - 1) / 3;
-                                m &= m - 1;
-#pragma unroll
-                                for (int rr = 0; rr < 6; ++rr) X[rr] += (r == rr) ? wq : 0.0;
-                            }
-                        }
-                    }
-                }
-            }
-            named_sync(1, 128);
-            {
-                const int jj = et >> 3, part = et & 7;
-                if (un.j0 + jj < un.bd.size2) {
-                    const int gj = un.bd.start2 + un.j0 + jj, cnt = a.misscnt[gj];
-                    const int *L = a.missidx + (size_t)gj * a.missstride;
-                    for (int q = part; q < cnt; q += 8) jbm[L[q] >> 1] = 0u;
-                }
-            }
-            named_sync(1, 128);
-
+            // sum of (ytilde^2 - qcen) over the individuals known at SNP i
+            const double pki = ivalid ? a.qtot[t] - a.qm[(size_t)t * a.nsnp + gi] : 0.0;
             if (!tc::mbar_wait(&sm.acc_full[buf], accph[buf], abort)) {
                 fail(a, sm, 3);
                 break;
             }
             tc::tc_fence_after();
-            const uint32_t acc = tl + (buf ? ACC_COL1 : 0);
+            // copy this lane's E row (48 columns) to shared memory and release the E accumulator
+            {
+                uint32_t ev[N2];
+                tc::tmem_ld16(tl + ACC_E, ev);
+                tc::tmem_ld16(tl + ACC_E + 16, ev + 16);
+                tc::tmem_ld16(tl + ACC_E + 32, ev + 32);
+                tc::tmem_wait_ld();
+                tc::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&sm.e_empty);
+#pragma unroll
+                for (int q = 0; q < N2 / 4; ++q)
+                    *reinterpret_cast<uint4 *>(&esum[lane][4 * q]) =
+                        make_uint4(ev[4 * q], ev[4 * q + 1], ev[4 * q + 2], ev[4 * q + 3]);
+                __syncwarp();
+            }
+            const uint32_t acc = tl + acc_col(buf);
             const bool report = a.report_trait < 0 || a.report_trait == t;
 #pragma unroll 1
             for (int rho = 0; rho < (TJ + 2) / 3; ++rho) {
                 const int jb = 3 * rho;
-                const int dj = un.j0 + jb + ga;
-                const bool valid = ivalid && (jb + ga < TJ) && dj < un.bd.size2 &&
+                const int jl = jb + ga;
+                const int dj = un.j0 + jl;
+                const bool valid = ivalid && (jl < TJ) && dj < un.bd.size2 &&
                                    (un.bd.start1 + di > un.bd.start2 + dj);
-                const int gj = un.bd.start2 + (valid ? dj : 0);
-                const double qmj = valid ? a.qm[(size_t)t * a.nsnp + gj] : 0.0;
-                uint32_t v[NTYPE][4];
+                const double rmj = valid ? a.rm[(size_t)t * a.nsnp + un.bd.start2 + dj] : 0.0;
+                uint32_t v[NTY][4];
 #pragma unroll
-                for (int ty = 0; ty < NTYPE; ++ty) tc::tmem_ld4(acc + ty * TJ + jb, v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
+                for (int ty = 0; ty < NTY; ++ty) tc::tmem_ld4(acc + ty * TJ + jb, v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
                 tc::tmem_wait_ld();
                 // rows (ii, a') for my j-SNP jb + ga: own row directly, the others by shuffle
-                uint32_t r1[NTYPE], r2[NTYPE];
+                uint32_t r1[NTY], r2[NTY];
 #pragma unroll
-                for (int ty = 0; ty < NTYPE; ++ty) {
+                for (int ty = 0; ty < NTY; ++ty) {
                     r1[ty] = __shfl_sync(0xffffffffu, sel3(v[ty], (ga + 2) % 3), tbase + (ga + 1) % 3);
                     r2[ty] = __shfl_sync(0xffffffffu, sel3(v[ty], (ga + 1) % 3), tbase + (ga + 2) % 3);
                 }
@@ -444,10 +435,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                                              65536LL * (long long)(int)c3;
                         }
                     }
-                    double xr = 0.0;
+                    int npair = 0;
 #pragma unroll
-                    for (int rr = 0; rr < 6; ++rr) xr = (rr == rho) ? X[rr] : xr;
-                    s = pair_stat_exact(n, si, sc, qtot - qmi - qmj + xr, a.test_int != 0);
+                    for (int c = 0; c < 9; ++c) npair += n[c];
+                    // E digit sums over individuals known at i (rows a = 0..2) and missing at j
+                    long long em = 0;
+#pragma unroll
+                    for (int ar = 0; ar < 3; ++ar)
+                        em += (long long)esum[tbase + ar][jl] + 256LL * (long long)esum[tbase + ar][TJ + jl] +
+                              65536LL * (long long)esum[tbase + ar][2 * TJ + jl];
+                    const double Q = fma(qcen, (double)npair, pki) - fma(qstep, (double)em, rmj);
+                    s = pair_stat_exact(n, si, sc, Q, a.test_int != 0);
                     if (t == a.report_trait && (a.dump_counts || a.dump_F)) {
                         const size_t o = (size_t)di * un.bd.size2 + dj;
                         if (a.dump_counts)
@@ -488,12 +486,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     tc::mbar_arrive_expect_tx(&sm.raw_full[rs], RAW_BYTES);
                     tc::tma_load_2d(raw + RAW_I, &maps.hi, ks * KS, un.bd.start1 + un.i0, &sm.raw_full[rs]);
                     tc::tma_load_2d(raw + RAW_J, &maps.hj, ks * KS, un.bd.start2 + un.j0, &sm.raw_full[rs]);
-                    tc::tma_load_2d(raw + RAW_D, &maps.dg, ks * KS, 4 * un.trait, &sm.raw_full[rs]);
+                    tc::tma_load_2d(raw + RAW_D, &maps.dg, ks * KS, ND * un.trait, &sm.raw_full[rs]);
                     ++issued;
-                    if (++rs == RSTAGES) {
-                        rs = 0;
-                        rph ^= 1u;
-                    }
+                    advance<RSTAGES>(rs, rph);
                 }
             }
             // no TMA write may still be landing in shared memory when the CTA exits: wait for
@@ -509,20 +504,22 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         }
     } else if (lane == 0) {
         // ---------------- MMA issuer ----------------
-        uint32_t stage = 0, phase = 0, accph[2] = {0u, 0u};
+        uint32_t stage = 0, phase = 0, as = 0, aph = 0, accph[2] = {0u, 0u}, eph = 0;
         int buf = 0;
         bool ok = true;
         for (long long u = blockIdx.x; u < units && ok; u += gridDim.x) {
             const Unit un = decode(a, u);
             if (un.skip) continue;
-            if (!tc::mbar_wait(&sm.acc_empty[buf], accph[buf] ^ 1u, abort)) {
+            if (!tc::mbar_wait(&sm.acc_empty[buf], accph[buf] ^ 1u, abort) ||
+                !tc::mbar_wait(&sm.e_empty, eph ^ 1u, abort)) {
                 fail(a, sm, 4);
                 break;
             }
+            eph ^= 1u;
             tc::tc_fence_after();
-            const uint32_t d = tmem + (buf ? ACC_COL1 : 0);
+            const uint32_t d = tmem + acc_col(buf);
             for (int ks = 0; ks < nks; ++ks) {
-                if (!tc::mbar_wait(&sm.full[stage], phase, abort)) {
+                if (!tc::mbar_wait(&sm.full[stage], phase, abort) || !tc::mbar_wait(&sm.afull[as], aph, abort)) {
                     fail(a, sm, 5);
                     ok = false;
                     break;
@@ -530,14 +527,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 tc::tc_fence_after();
                 const uint32_t bs = tc::smem_u32(sm.b[stage]);
 #pragma unroll
-                for (int kk = 0; kk < KS / 32; ++kk)
-                    tc::mma_i8_ts(d, tmem + A_COL + 32 * stage + 8 * kk, tc::smem_desc_sw128(bs + 32 * kk), IDESC,
+                for (int kk = 0; kk < KS / 32; ++kk) {
+                    const uint32_t at = tmem + a_col(as) + 8 * kk;
+                    tc::mma_i8_ts(d, at, tc::smem_desc_sw128(bs + 32 * kk), IDESC1, (ks | kk) != 0);
+                    tc::mma_i8_ts(tmem + ACC_E, at, tc::smem_desc_sw128(bs + N1 * 128 + 32 * kk), IDESC2,
                                   (ks | kk) != 0);
-                tc::mma_commit(&sm.empty[stage]);
-                if (++stage == STAGES) {
-                    stage = 0;
-                    phase ^= 1u;
                 }
+                tc::mma_commit(&sm.empty[stage]);
+                tc::mma_commit(&sm.aempty[as]);
+                advance<STAGES>(stage, phase);
+                advance<ASTAGES>(as, aph);
             }
             if (!ok) break;
             tc::mma_commit(&sm.acc_full[buf]);
@@ -564,7 +563,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
 }  // namespace mma
 
 // Tensor maps of the tensor form's TMA loads: the one-hot genotype bytes [nsnp][Np] with
-// boxes of 40 and 16 rows x 128 bytes, and the trait digit rows [4T][Np] with 4-row boxes;
+// boxes of 40 and 16 rows x 128 bytes, and the trait digit rows [7T][Np] with 7-row boxes;
 // all 128-byte swizzled, out-of-range rows read as zero.
 static cudaError_t encode_2d(CUtensorMap *m, const void *base, uint64_t inner, uint64_t rows, uint32_t box_rows)
 {
@@ -595,21 +594,21 @@ cudaError_t mma_encode_genotypes(MmaMaps *maps, const uint8_t *hcodes, int nsnp,
 
 cudaError_t mma_encode_traits(MmaMaps *maps, const int8_t *ydig, int ntraits, int Np)
 {
-    return encode_2d(&maps->dg, ydig, (uint64_t)Np, (uint64_t)4 * ntraits, 4);
+    return encode_2d(&maps->dg, ydig, (uint64_t)Np, (uint64_t)mma::ND * ntraits, mma::ND);
 }
 
 bool mma_available() { return true; }
 int mma_tile_i() { return mma::TI; }
 int mma_tile_j() { return mma::TJ; }
 int mma_min_nid() { return 256; }
-int mma_max_nid() { return mma::MAX_NP; }
+int mma_max_nid() { return 1 << 24; }  // digit sums stay within int32
 int mma_stage_individuals() { return mma::KS; }
 
 cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream)
 {
     // more than half of the SM's shared memory: one CTA per SM, which owns all 512 TMEM columns;
-    // the tail holds the epilogue's missing bitmap, 2 bytes per individual
-    const size_t smem = sizeof(mma::Smem) + 1024 + (size_t)a.Np * 2 + 8 * (size_t)a.ntraits;
+    // the tail holds the per-CTA maxima
+    const size_t smem = sizeof(mma::Smem) + 1024 + 8 * (size_t)a.ntraits;
     static_assert(sizeof(mma::Smem) + 1024 > 116 * 1024, "one CTA per SM");
     cudaError_t e = cudaFuncSetAttribute(mma::k_scan_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

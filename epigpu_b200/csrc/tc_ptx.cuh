@@ -155,6 +155,18 @@ __device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t &a, uint32_t &
                  : "memory");
 }
 
+// 32 lanes x 16 consecutive 32-bit columns: thread t reads lane (base lane + t) into v[0..15].
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t v[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                 "%13, %14, %15}, [%16];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                   "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                   "=r"(v[15])
+                 : "r"(taddr)
+                 : "memory");
+}
+
 // Shared-memory matrix descriptor for a K-major operand in the 128-byte swizzled
 // canonical layout: rows of 128 bytes, 8-row groups 1024 bytes apart (SBO), version 1.
 __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr)

@@ -47,3 +47,28 @@ def test_f_error_at_n10000(gpu_ctx, data, form):
     print("\nF error vs FP64, form %d, N=%d, %d pairs: 8df rel max %.3g median %.3g (%d pairs F>=1), abs max "
           "%.3g below; 4df rel max %.3g median %.3g (%d pairs), abs max %.3g below"
           % (form, NID, tri.sum(), *out["F"], *out["F2"]))
+
+
+@pytest.mark.parametrize("form", [capi.FORM_POPC, capi.FORM_TENSOR], ids=["popc", "tensor"])
+def test_f_error_low_call_rate_individuals(gpu_ctx, form):
+    """Missingness concentrated in a few individuals (48 of 2,000 miss half of all SNPs, the
+    rest 0.5%), so most pairs share individuals missing at both SNPs, with a skewed trait
+    and one far outlier (a large y^2 range). Every pair within the 1e-5 bar, counts exact."""
+    nid, nsnp = 2000, 300
+    rng = np.random.default_rng(61)
+    codes = synth.genotype_codes(nid, nsnp, seed=62, miss=0.005)
+    low = rng.choice(nid, 48, replace=False)
+    codes[:, low] = np.where(rng.random((nsnp, low.size)) < 0.5, 3, codes[:, low])
+    y = ((rng.gamma(1.5, 1.0, nid) - 1.5)).astype(np.float32)
+    y[low[0]] = 25.0
+    phen = np.where(rng.random(nid) < 0.02, np.float32(-9.0), y).astype(np.float32)
+    blk = (0, nsnp, 0, nsnp)
+    hb, tb, pb = oracles.oracle_scan_block(codes, phen, blk, test="i", t1=-1e30, t2=-1e30, per_pair=True)
+    gpu_ctx.load_packed(synth.pack(codes), nid)
+    gpu_ctx.set_phenotype(phen)
+    d = gpu_ctx.scan_dump(blk, capi.default_opts(test="i", t1=-1e30, t2=-1e30, form=form))
+    tri = np.tril(np.ones((nsnp, nsnp), bool), -1)
+    assert np.array_equal(d["counts"][tri], pb["counts"][tri])
+    for field in ("F", "F2"):
+        ref, got = pb[field][tri], d[field][tri].astype(np.float64)
+        assert parity.f_excess(got, ref, pb["df1"][tri], pb["df2"][tri], 1e-5).max() <= 1.0, field
