@@ -35,6 +35,8 @@ WORKLOADS = {
     "cfg3": (10000, [100000], "i", 1, "8 df + 4 df scan, N=10,000 individuals, M=100,000 SNPs, 1 chromosome"),
     "cfg4": (5000, [50000], "f", 64, "8 df scan, N=5,000, M=50,000, 64 phenotype columns (permutations)"),
     "cfg5": (8000, None, "f", 8, "8 df scan, N=8,000, 22 uneven blocks (M=250,000), 8 traits with own masks"),
+    # the cfg3 kernel on a block small enough for an ncu capture of one launch
+    "cfg3s": (10000, [4000], "i", 1, "8 df + 4 df scan, N=10,000 individuals, M=4,000 SNPs (profiling size)"),
 }
 
 

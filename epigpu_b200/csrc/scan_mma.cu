@@ -3,17 +3,16 @@
 // Per pair (i, j) the reference accumulates, over individuals k, the 3x3 genotype-cell
 // counts and phenotype sums (src/EpiOpenCL.c:110-228). Both are contractions over k:
 //     n_ab = sum_k [g_i(k)=a] [g_j(k)=b] w_k        S_ab = sum_k [g_i(k)=a] [g_j(k)=b] y_k
-// so for a tile of 40 i-SNPs x 16 j-SNPs they are one integer GEMM
-//     D[128 x 240] = A[128 x K] * B[K x 240]
+// so for a tile of 40 i-SNPs x 14 j-SNPs they are one integer GEMM
+//     D[128 x 224] = A[128 x K] * B[K x 224]
 //   A rows (TMEM lane 32w + l, l < 30): i-SNP 10w + l/3, genotype a = l%3: [g_i(k) == a]
-//   B cols (type t, column 16t + j'):
+//   B cols (type t, column 14t + j'; columns 210-223 are zero):
 //     t = 4b + s (t < 12): [g_j(k) == b] * D_s(k), D_0 = w_k (phenotype valid) and D_1..3 the
 //       balanced base-256 digits of the fixed-point phenotype Y_k = round(y_k * 2^sy)
 //       (y centred, 0 when invalid);
 //     t = 12..14: [g_j(k) missing] * E_s(k), the three balanced digits of
 //       E_k = round((ytilde_k^2 - qcen) / qstep), ytilde = Y 2^-sy (0 when invalid).
-// issued as two MMAs per K step: columns 0-191 into a double-buffered accumulator, columns
-// 192-239 (the E sums) into a single one that the epilogue copies to shared memory first.
+// issued as one N = 224 MMA per 32 individuals into one of two accumulators.
 // int8 operands, int32 accumulation: counts and digit sums are exact, so
 //     S_ab = (D1 + 256 D2 + 65536 D3) * 2^-sy exactly for the quantised phenotype.
 // The sum of ytilde^2 over the pair's valid individuals (both genotypes known, phenotype
@@ -29,21 +28,22 @@
 // Persistent kernel, one CTA per SM, warp-specialised, 14 warps:
 //   warp 13     TMA loader (one thread): per 128-individual stage, three 2-D tiled loads
 //               (no multicast) into a 6-deep raw ring: the i-tile's and j-tile's one-hot
-//               genotype bytes (40 and 16 rows x 128 B) and the trait's 6 digit rows,
+//               genotype bytes (40 and 14 rows x 128 B) and the trait's 7 digit rows,
 //               128-byte swizzled; completion by mbarrier transaction bytes
 //   warps 0-3   A producers: one TMEM lane each; expand the raw i rows into the stage's A
 //               rows and store them into TMEM with tcgen05.st (the MMA reads A from TMEM)
 //   warps 4-7   B producers: expand raw j rows x digits into the stage's B tile (K-major,
 //               128-byte swizzle) in smem
-//   warps 8-11  epilogue: copy of the E accumulator to shared memory, tcgen05.ld of the
-//               main accumulator, lane-triplet shuffles, FP64 statistics, warp-aggregated
-//               hit append, per-trait max F
-//   warp 12     TMEM allocator and MMA issuer (one thread): 8 x tcgen05.mma per stage
-// TMEM (512 columns): accumulators 0 and 1 at [0, 192) and [192, 384), the E accumulator at
-// [384, 432), A stages at [432, 464) and [464, 496). 4-stage B ring, 2-stage A ring, 2 main
-// accumulators, so the epilogue of one tile overlaps the MMAs of the next (which wait only for
-// the short E copy). All waits are bounded (tc_ptx.cuh); a timeout sets counters[2] and every
-// role leaves its loop.
+//   warps 8-11  epilogue: tcgen05.ld of the accumulator, lane-triplet shuffles, FP64
+//               statistics, warp-aggregated hit append, per-trait max F
+//   warp 12     TMEM allocator and MMA issuer (one thread): 4 x tcgen05.mma per stage
+// TMEM (512 columns): accumulators at [0, 224) and [224, 448), two A stages of 128
+// individuals (32 columns) at [448, 512). An M = 128, K = 32 int8 MMA takes nearly the same
+// time for any N from 192 to 256, so one wide instruction carries every column type; the j
+// tile is 14 SNPs so that two accumulators and two A stages fit the TMEM. 4-stage B ring,
+// 2-stage A ring, 2 accumulators, so the epilogue of one tile overlaps the MMAs of the next.
+// All waits are bounded (tc_ptx.cuh); a timeout sets counters[2] and every role leaves its
+// loop.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -54,43 +54,39 @@ namespace epi {
 namespace mma {
 
 constexpr int TI = 40;         // i-SNPs per tile (4 warps x 10 lane triplets)
-constexpr int TJ = 16;         // j-SNPs per tile
-constexpr int NTY = 12;        // main B column types per j-SNP: b (3) x {w, d0, d1, d2}
-constexpr int NE = 3;          // E column types per j-SNP: missing x {e0, e1, e2}
-constexpr int N1 = TJ * NTY;   // 192
-constexpr int N2 = TJ * NE;    // 48
-constexpr int NB = N1 + N2;    // B tile rows (240)
+constexpr int TJ = 14;         // j-SNPs per tile
+constexpr int NTY = 12;        // B column types per j-SNP: b (3) x {w, d0, d1, d2} ...
+constexpr int NTYPE = 15;      // ... and missing x {e0, e1, e2}
+constexpr int NCOL = TJ * NTYPE;           // 210 columns in use
+constexpr int N = (NCOL + 15) / 16 * 16;  // 224: MMA width (padding columns are zero)
 constexpr int M = 128;
 constexpr int KS = 128;        // individuals per pipeline stage
 constexpr int STAGES = 4;      // B ring (smem)
 constexpr int ASTAGES = 2;     // A ring (TMEM)
 constexpr int ND = 7;          // digit rows per trait: w, Y digits (3), E digits (3)
-constexpr uint32_t ACC_COL0 = 0, ACC_COL1 = 192, ACC_E = 384, A_COL0 = 432, A_COL1 = 464;
-constexpr int ESTRIDE = 52;    // words per lane row of the E copy in smem (48 used)
-__host__ __device__ constexpr uint32_t acc_col(uint32_t buf) { return buf ? ACC_COL1 : ACC_COL0; }
-__host__ __device__ constexpr uint32_t a_col(uint32_t s) { return s ? A_COL1 : A_COL0; }
+constexpr uint32_t ACC_COL1 = N, A_COL = 2 * N;
+__host__ __device__ constexpr uint32_t acc_col(uint32_t buf) { return buf ? ACC_COL1 : 0u; }
+__host__ __device__ constexpr uint32_t a_col(uint32_t s) { return A_COL + 32 * s; }
 constexpr uint32_t TMEM_COLS = 512;
-constexpr int B_STAGE = NB * KS;  // bytes per B stage (30 KB)
+constexpr int B_STAGE = N * KS;  // bytes per B stage (30 KB)
 constexpr int RSTAGES = 6;       // raw (TMA) ring depth
 // raw stage: one-hot genotype rows (40 i, 16 j) and the trait's digit rows
-constexpr int RAW_I = 0, RAW_J = TI * KS, RAW_D = RAW_J + TJ * KS;
+constexpr int RAW_I = 0, RAW_J = TI * KS, RAW_D = RAW_J + 16 * KS;  // 1024-aligned sections
 constexpr int RAW_STAGE = 8 * 1024;
 constexpr uint32_t RAW_BYTES = (TI + TJ + ND) * KS;  // transaction bytes per raw stage
 constexpr int NWARPS = 14;
 constexpr int NTHREADS = NWARPS * 32;
-constexpr uint32_t IDESC1 = tc::idesc_i8(M, N1), IDESC2 = tc::idesc_i8(M, N2);
-static_assert(RAW_J % 1024 == 0 && RAW_D % 1024 == 0 && RAW_D + ND * KS <= RAW_STAGE, "raw layout");
-static_assert(B_STAGE % 1024 == 0 && (N1 * KS) % 1024 == 0 && N1 % 16 == 0 && N2 % 16 == 0, "B tile");
-static_assert(ASTAGES == 2 && ACC_COL0 + N1 <= ACC_COL1 && ACC_COL1 + N1 <= ACC_E && ACC_E + N2 <= A_COL0 &&
-                  A_COL0 + KS / 4 <= A_COL1 && A_COL1 + KS / 4 <= TMEM_COLS,
-              "TMEM layout");
+constexpr uint32_t IDESC = tc::idesc_i8(M, N);
+static_assert(RAW_J % 1024 == 0 && RAW_D % 1024 == 0 && RAW_J + TJ * KS <= RAW_D && RAW_D + ND * KS <= RAW_STAGE,
+              "raw layout");
+static_assert(B_STAGE % 1024 == 0 && N % 16 == 0 && N <= 256, "B tile");
+static_assert(a_col(ASTAGES - 1) + KS / 4 <= TMEM_COLS, "TMEM layout");
 
 struct Smem {
     uint8_t b[STAGES][B_STAGE];
     uint8_t raw[RSTAGES][RAW_STAGE];
-    int32_t esum[4 * 32][ESTRIDE];  // per TMEM lane: the tile's E accumulator row
     uint64_t full[STAGES], empty[STAGES], afull[ASTAGES], aempty[ASTAGES], raw_full[RSTAGES], raw_empty[RSTAGES],
-        acc_full[2], acc_empty[2], e_empty, drain;
+        acc_full[2], acc_empty[2], drain;
     uint32_t tmem_base;
     int abort;
 };
@@ -222,6 +218,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         tc::tmem_alloc(&sm.tmem_base, TMEM_COLS);
         tc::tmem_relinquish();
     }
+    // the B padding rows (columns NCOL..N-1 of every stage) are never written by the producers
+    for (int w = threadIdx.x; w < STAGES * (N - NCOL) * 8; w += blockDim.x) {
+        const int st = w / ((N - NCOL) * 8), n = NCOL + (w / 8) % (N - NCOL), c = w % 8;
+        *reinterpret_cast<uint4 *>(sm.b[st] + (n >> 3) * 1024 + (n & 7) * 128 + c * 16) = make_uint4(0, 0, 0, 0);
+    }
+    tc::fence_proxy_async_smem();
     // per-CTA maxima of F and F2 per trait (flushed to global memory once, at the end)
     unsigned int *smax = reinterpret_cast<unsigned int *>(reinterpret_cast<uint8_t *>(&sm) + sizeof(Smem));
     for (int w = threadIdx.x; w < 2 * a.ntraits; w += blockDim.x) smax[w] = 0u;
@@ -242,7 +244,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             tc::mbar_init(&sm.acc_full[b], 1);
             tc::mbar_init(&sm.acc_empty[b], 4);
         }
-        tc::mbar_init(&sm.e_empty, 4);
         tc::mbar_init(&sm.drain, 1);
         sm.abort = 0;
         tc::fence_barrier_init();
@@ -263,8 +264,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         for (long long u = blockIdx.x; u < units && ok; u += gridDim.x) {
             const Unit un = decode(a, u);
             if (un.skip) continue;
-            for (int ks = 0; ks < nks; ++ks) {
-                if (!tc::mbar_wait(&sm.raw_full[rs], rph, abort) || !tc::mbar_wait(&sm.aempty[as], aph ^ 1u, abort)) {
+            for (int ks = 0; ks < nks && ok; ++ks) {
+                if (!tc::mbar_wait(&sm.raw_full[rs], rph, abort)) {
                     fail(a, sm, 1);
                     ok = false;
                     break;
@@ -279,15 +280,21 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     v[4 * c + 2] = (h.z >> ga) & 0x01010101u;
                     v[4 * c + 3] = (h.w >> ga) & 0x01010101u;
                 }
+                if (!tc::mbar_wait(&sm.aempty[as], aph ^ 1u, abort)) {
+                    fail(a, sm, 1);
+                    ok = false;
+                    break;
+                }
+                tc::tmem_st32(taddr_lane + a_col(as), v);
+                // the raw slot is released after the store, which consumes every loaded value
                 __syncwarp();
                 if (lane == 0) tc::mbar_arrive(&sm.raw_empty[rs]);
-                tc::tmem_st32(taddr_lane + a_col(as), v);
+                advance<RSTAGES>(rs, rph);
                 tc::tmem_wait_st();
                 tc::tc_fence_before();
                 __syncwarp();
                 if (lane == 0) tc::mbar_arrive(&sm.afull[as]);
                 advance<ASTAGES>(as, aph);
-                advance<RSTAGES>(rs, rph);
             }
         }
     } else if (warp < 8) {
@@ -305,14 +312,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     break;
                 }
                 const uint8_t *raw = sm.raw[rs];
-                const uint4 h = ld_sw128(raw + RAW_J, jj, c);
+                const bool jok = jj < TJ;  // threads 112-127 have no j row
+                const uint4 h = jok ? ld_sw128(raw + RAW_J, jj, c) : make_uint4(0, 0, 0, 0);
                 uint4 d[ND];
 #pragma unroll
                 for (int s2 = 0; s2 < ND; ++s2) d[s2] = ld_sw128(raw + RAW_D, s2, c);
-                __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&sm.raw_empty[rs]);
                 uint8_t *base = sm.b[stage];
                 auto put = [&](int ty, const uint4 &m, const uint4 &dv) {
+                    if (!jok) return;
                     const int n = ty * TJ + jj;
                     uint4 o;
                     o.x = m.x & dv.x;
@@ -341,9 +348,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 put(12, mm, d[4]);
                 put(13, mm, d[5]);
                 put(14, mm, d[6]);
+                // the raw slot is released only after the stores above, which consume every
+                // value loaded from it (an arrive right after the loads can overtake them)
                 tc::fence_proxy_async_smem();
                 __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&sm.full[stage]);
+                if (lane == 0) {
+                    tc::mbar_arrive(&sm.raw_empty[rs]);
+                    tc::mbar_arrive(&sm.full[stage]);
+                }
                 advance<STAGES>(stage, phase);
                 advance<RSTAGES>(rs, rph);
             }
@@ -354,7 +366,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         const int ii = 10 * e + lane / 3, ga = lane % 3, tbase = (lane / 3) * 3;
         const bool rowok = lane < 30;
         const uint32_t tl = tmem + ((uint32_t)(32 * e) << 16);
-        int32_t(*esum)[ESTRIDE] = sm.esum + 32 * e;  // this warp's 32 lane rows
         uint32_t accph[2] = {0u, 0u};
         int buf = 0;
         for (long long u = blockIdx.x; u < units; u += gridDim.x) {
@@ -372,22 +383,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 break;
             }
             tc::tc_fence_after();
-            // copy this lane's E row (48 columns) to shared memory and release the E accumulator
-            {
-                uint32_t ev[N2];
-                tc::tmem_ld16(tl + ACC_E, ev);
-                tc::tmem_ld16(tl + ACC_E + 16, ev + 16);
-                tc::tmem_ld16(tl + ACC_E + 32, ev + 32);
-                tc::tmem_wait_ld();
-                tc::tc_fence_before();
-                __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&sm.e_empty);
-#pragma unroll
-                for (int q = 0; q < N2 / 4; ++q)
-                    *reinterpret_cast<uint4 *>(&esum[lane][4 * q]) =
-                        make_uint4(ev[4 * q], ev[4 * q + 1], ev[4 * q + 2], ev[4 * q + 3]);
-                __syncwarp();
-            }
             const uint32_t acc = tl + acc_col(buf);
             const bool report = a.report_trait < 0 || a.report_trait == t;
 #pragma unroll 1
@@ -398,14 +393,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 const bool valid = ivalid && (jl < TJ) && dj < un.bd.size2 &&
                                    (un.bd.start1 + di > un.bd.start2 + dj);
                 const double rmj = valid ? a.rm[(size_t)t * a.nsnp + un.bd.start2 + dj] : 0.0;
-                uint32_t v[NTY][4];
+                uint32_t v[NTYPE][4];
 #pragma unroll
-                for (int ty = 0; ty < NTY; ++ty) tc::tmem_ld4(acc + ty * TJ + jb, v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
+                for (int ty = 0; ty < NTYPE; ++ty)
+                    tc::tmem_ld4(acc + ty * TJ + jb, v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
                 tc::tmem_wait_ld();
                 // rows (ii, a') for my j-SNP jb + ga: own row directly, the others by shuffle
-                uint32_t r1[NTY], r2[NTY];
+                uint32_t r1[NTYPE], r2[NTYPE];
 #pragma unroll
-                for (int ty = 0; ty < NTY; ++ty) {
+                for (int ty = 0; ty < NTYPE; ++ty) {
                     r1[ty] = __shfl_sync(0xffffffffu, sel3(v[ty], (ga + 2) % 3), tbase + (ga + 1) % 3);
                     r2[ty] = __shfl_sync(0xffffffffu, sel3(v[ty], (ga + 1) % 3), tbase + (ga + 2) % 3);
                 }
@@ -441,9 +437,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     // E digit sums over individuals known at i (rows a = 0..2) and missing at j
                     long long em = 0;
 #pragma unroll
-                    for (int ar = 0; ar < 3; ++ar)
-                        em += (long long)esum[tbase + ar][jl] + 256LL * (long long)esum[tbase + ar][TJ + jl] +
-                              65536LL * (long long)esum[tbase + ar][2 * TJ + jl];
+                    for (int d = 0; d < 3; ++d) {
+                        const long long sd = (long long)(int)sel3(v[NTY + d], ga) + (long long)(int)r1[NTY + d] +
+                                             (long long)(int)r2[NTY + d];
+                        em += sd * (1LL << (8 * d));
+                    }
                     const double Q = fma(qcen, (double)npair, pki) - fma(qstep, (double)em, rmj);
                     s = pair_stat_exact(n, si, sc, Q, a.test_int != 0);
                     if (t == a.report_trait && (a.dump_counts || a.dump_F)) {
@@ -504,18 +502,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         }
     } else if (lane == 0) {
         // ---------------- MMA issuer ----------------
-        uint32_t stage = 0, phase = 0, as = 0, aph = 0, accph[2] = {0u, 0u}, eph = 0;
+        uint32_t stage = 0, phase = 0, as = 0, aph = 0, accph[2] = {0u, 0u};
         int buf = 0;
         bool ok = true;
         for (long long u = blockIdx.x; u < units && ok; u += gridDim.x) {
             const Unit un = decode(a, u);
             if (un.skip) continue;
-            if (!tc::mbar_wait(&sm.acc_empty[buf], accph[buf] ^ 1u, abort) ||
-                !tc::mbar_wait(&sm.e_empty, eph ^ 1u, abort)) {
+            if (!tc::mbar_wait(&sm.acc_empty[buf], accph[buf] ^ 1u, abort)) {
                 fail(a, sm, 4);
                 break;
             }
-            eph ^= 1u;
             tc::tc_fence_after();
             const uint32_t d = tmem + acc_col(buf);
             for (int ks = 0; ks < nks; ++ks) {
@@ -527,12 +523,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 tc::tc_fence_after();
                 const uint32_t bs = tc::smem_u32(sm.b[stage]);
 #pragma unroll
-                for (int kk = 0; kk < KS / 32; ++kk) {
-                    const uint32_t at = tmem + a_col(as) + 8 * kk;
-                    tc::mma_i8_ts(d, at, tc::smem_desc_sw128(bs + 32 * kk), IDESC1, (ks | kk) != 0);
-                    tc::mma_i8_ts(tmem + ACC_E, at, tc::smem_desc_sw128(bs + N1 * 128 + 32 * kk), IDESC2,
+                for (int kk = 0; kk < KS / 32; ++kk)
+                    tc::mma_i8_ts(d, tmem + a_col(as) + 8 * kk, tc::smem_desc_sw128(bs + 32 * kk), IDESC,
                                   (ks | kk) != 0);
-                }
                 tc::mma_commit(&sm.empty[stage]);
                 tc::mma_commit(&sm.aempty[as]);
                 advance<STAGES>(stage, phase);
