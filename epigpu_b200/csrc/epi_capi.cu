@@ -20,7 +20,8 @@
 
 namespace epi {
 cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int remain, uint4 *planes, int Wp,
-                          uint32_t *codes, int Wc, uint8_t *hcodes, uint32_t *missbits, cudaStream_t stream);
+                          uint32_t *codes, int Wc, uint8_t *hcodes, uint8_t *h3, uint32_t *missbits,
+                          cudaStream_t stream);
 cudaError_t launch_qmiss(const uint32_t *missbits, int nsnp, int Wp, const uint32_t *wmask, const double *qd,
                         const double *qr, int Np, int ntraits, double *qm, double *rm, cudaStream_t stream);
 cudaError_t launch_popc(const ScanArgs &a, int grid, cudaStream_t stream);
@@ -33,7 +34,7 @@ int mma_tile_j();
 int mma_min_nid();
 int mma_max_nid();
 cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream);
-cudaError_t mma_encode_genotypes(MmaMaps *maps, const uint8_t *hcodes, int nsnp, int Np);
+cudaError_t mma_encode_genotypes(MmaMaps *maps, const uint8_t *hcodes, const uint8_t *h3, int nsnp, int Np);
 cudaError_t mma_encode_traits(MmaMaps *maps, const int8_t *ydig, int ntraits, int Np);
 }  // namespace epi
 
@@ -52,9 +53,9 @@ struct epi_ctx {
     int32_t *d_raw = nullptr;
     size_t raw_cap = 0;
     uint4 *d_planes = nullptr;
-    uint8_t *d_hcodes = nullptr;
+    uint8_t *d_hcodes = nullptr, *d_h3 = nullptr;
     uint32_t *d_missbits = nullptr;
-    size_t planes_cap = 0, hcodes_cap = 0, missbits_cap = 0;
+    size_t planes_cap = 0, hcodes_cap = 0, h3_cap = 0, missbits_cap = 0;
     // traits
     int ntraits = 0, traits_nid = 0;
     float *d_y = nullptr, *d_q = nullptr;
@@ -179,7 +180,7 @@ epi_status epi_close(epi_ctx *ctx)
     if (!ctx) return EPI_OK;
     if (ctx->device >= 0) cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    void *bufs[] = {ctx->d_raw, ctx->d_planes, ctx->d_hcodes, ctx->d_missbits, ctx->d_y, ctx->d_q,
+    void *bufs[] = {ctx->d_raw, ctx->d_planes, ctx->d_hcodes, ctx->d_h3, ctx->d_missbits, ctx->d_y, ctx->d_q,
                     ctx->d_wmask, ctx->d_qc, ctx->d_yscale, ctx->d_qd, ctx->d_qtot, ctx->d_qm, ctx->d_ydig,
                     ctx->d_hits, ctx->d_counters, ctx->d_maxf, ctx->d_blocks};
     for (void *p : bufs)
@@ -215,13 +216,14 @@ epi_status epi_load_packed(epi_ctx *ctx, const int32_t *gpack, int32_t nid, int3
     CK(ensure(&ctx->d_raw, &ctx->raw_cap, (size_t)nsnp * npack1 * sizeof(int32_t)));
     CK(ensure(&ctx->d_planes, &ctx->planes_cap, (size_t)nsnp * Wp * sizeof(uint4)));
     CK(ensure(&ctx->d_hcodes, &ctx->hcodes_cap, (size_t)nsnp * Wp * 32));
+    CK(ensure(&ctx->d_h3, &ctx->h3_cap, 3 * (size_t)nsnp * Wp * 32));
     CK(ensure(&ctx->d_missbits, &ctx->missbits_cap, (size_t)nsnp * Wp * sizeof(uint32_t)));
     CK(cudaMemcpyAsync(ctx->d_raw, gpack, (size_t)nsnp * npack1 * sizeof(int32_t), cudaMemcpyHostToDevice,
                        ctx->stream));
     CK(epi::launch_unpack(ctx->d_raw, nsnp, nid, npack, remain, ctx->d_planes, Wp, nullptr, Wc, ctx->d_hcodes,
-                          ctx->d_missbits, ctx->stream));
+                          ctx->d_h3, ctx->d_missbits, ctx->stream));
     ctx->qm_valid = false;
-    CK(epi::mma_encode_genotypes(&ctx->maps, ctx->d_hcodes, nsnp, 32 * Wp));
+    CK(epi::mma_encode_genotypes(&ctx->maps, ctx->d_hcodes, ctx->d_h3, nsnp, 32 * Wp));
     if (ctx->traits_nid != nid) ctx->ntraits = 0;  // traits no longer match
     ctx->nid = nid;
     ctx->nsnp = nsnp;

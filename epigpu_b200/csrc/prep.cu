@@ -20,10 +20,11 @@ __device__ __forceinline__ uint32_t ref_code(const int32_t *row, int k, int nid,
 }
 
 // One thread per (SNP, 32-individual word). Also writes the tensor form's one-hot code
-// bytes (1 << g, 0 when missing or padding) and missing-genotype bits.
+// bytes (1 << g, 0 when missing or padding), its genotype-indicator rows h3 (row 3s + a holds
+// the byte [g == a] per individual) and the missing-genotype bits.
 __global__ void k_unpack(const int32_t *__restrict__ raw, int nsnp, int nid, int npack, int remain,
                          int npack1, uint4 *__restrict__ planes, int Wp, uint32_t *__restrict__ codes, int Wc,
-                         uint8_t *__restrict__ hcodes, uint32_t *__restrict__ missbits)
+                         uint8_t *__restrict__ hcodes, uint8_t *__restrict__ h3, uint32_t *__restrict__ missbits)
 {
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long total = (long long)nsnp * Wp;
@@ -49,6 +50,18 @@ __global__ void k_unpack(const int32_t *__restrict__ raw, int nsnp, int nid, int
         uint4 *dst = reinterpret_cast<uint4 *>(hcodes + ((size_t)s * Wp + w) * 32);
         dst[0] = make_uint4(h[0], h[1], h[2], h[3]);
         dst[1] = make_uint4(h[4], h[5], h[6], h[7]);
+    }
+    if (h3 != nullptr) {
+        const size_t Np = (size_t)Wp * 32;
+#pragma unroll
+        for (int g = 0; g < 3; ++g) {
+            uint32_t e[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) e[q] = (h[q] >> g) & 0x01010101u;
+            uint4 *dst = reinterpret_cast<uint4 *>(h3 + (3 * (size_t)s + g) * Np + (size_t)w * 32);
+            dst[0] = make_uint4(e[0], e[1], e[2], e[3]);
+            dst[1] = make_uint4(e[4], e[5], e[6], e[7]);
+        }
     }
     if (missbits != nullptr) missbits[(size_t)s * Wp + w] = miss;
     if (codes != nullptr) {
@@ -82,14 +95,15 @@ __global__ void k_qmiss(const uint32_t *__restrict__ missbits, int nsnp, int Wp,
 }
 
 cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int remain, uint4 *planes, int Wp,
-                          uint32_t *codes, int Wc, uint8_t *hcodes, uint32_t *missbits, cudaStream_t stream)
+                          uint32_t *codes, int Wc, uint8_t *hcodes, uint8_t *h3, uint32_t *missbits,
+                          cudaStream_t stream)
 {
     const int npack1 = remain ? npack + 1 : npack;
     const long long total = (long long)nsnp * Wp;
     const int nt = 256;
     const long long nb = (total + nt - 1) / nt;
     k_unpack<<<(unsigned)nb, nt, 0, stream>>>(raw, nsnp, nid, npack, remain, npack1, planes, Wp, codes, Wc, hcodes,
-                                              missbits);
+                                              h3, missbits);
     return cudaGetLastError();
 }
 

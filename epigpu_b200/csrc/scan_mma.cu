@@ -3,47 +3,47 @@
 // Per pair (i, j) the reference accumulates, over individuals k, the 3x3 genotype-cell
 // counts and phenotype sums (src/EpiOpenCL.c:110-228). Both are contractions over k:
 //     n_ab = sum_k [g_i(k)=a] [g_j(k)=b] w_k        S_ab = sum_k [g_i(k)=a] [g_j(k)=b] y_k
-// so for a tile of 40 i-SNPs x 14 j-SNPs they are one integer GEMM
-//     D[128 x 224] = A[128 x K] * B[K x 224]
-//   A rows (TMEM lane 32w + l, l < 30): i-SNP 10w + l/3, genotype a = l%3: [g_i(k) == a]
-//   B cols (type t, column 14t + j'; columns 210-223 are zero):
+// so for a tile of 40 i-SNPs x 16 j-SNPs they are one integer GEMM
+//     D[128 x 240] = A[128 x K] * B[K x 240]
+//   A rows (row 32w + l, l < 30): i-SNP 10w + l/3, genotype a = l%3: [g_i(k) == a]
+//   B cols (type t, column 16t + j'):
 //     t = 4b + s (t < 12): [g_j(k) == b] * D_s(k), D_0 = w_k (phenotype valid) and D_1..3 the
 //       balanced base-256 digits of the fixed-point phenotype Y_k = round(y_k * 2^sy)
 //       (y centred, 0 when invalid);
 //     t = 12..14: [g_j(k) missing] * E_s(k), the three balanced digits of
 //       E_k = round((ytilde_k^2 - qcen) / qstep), ytilde = Y 2^-sy (0 when invalid).
-// issued as one N = 224 MMA per 32 individuals into one of two accumulators.
 // int8 operands, int32 accumulation: counts and digit sums are exact, so
 //     S_ab = (D1 + 256 D2 + 65536 D3) * 2^-sy exactly for the quantised phenotype.
 // The sum of ytilde^2 over the pair's valid individuals (both genotypes known, phenotype
 // valid) is, with e_k = ytilde_k^2 - qcen = qstep E_k + r_k,
 //     Q_ij = qcen * N_ij + (qtot - QM_i) - sum_k [g_i(k) known] [g_j(k) missing] e_k
 // where qtot - QM_i = sum of e over individuals known at i (exact FP64, per SNP), and the
-// last sum is qstep times the t = 12, 13 columns summed over a, plus the residuals r over the
+// last sum is qstep times the t = 12..14 columns summed over a, plus the residuals r over the
 // same individuals, taken as RM_j (r summed over all individuals missing at j, FP64, per
 // SNP). The one approximation: the residuals of individuals missing at both SNPs are counted
 // in RM_j, an error of at most qstep / 2 per such individual (qstep = max(ytilde^2) / 2^24).
 // The epilogue forms SSB / SSI / F / F2 in FP64.
 //
+// A comes straight from HBM: the genotype-indicator rows h3 (row 3s + a = [g_s == a] bytes)
+// are TMA-loaded into a 128-byte-swizzled shared-memory stage and read by the MMA from there
+// (no register pass). B is expanded from the j-tile's one-hot genotype bytes and the trait's
+// digit rows by producer warps.
+//
 // Persistent kernel, one CTA per SM, warp-specialised, 14 warps:
-//   warp 13     TMA loader (one thread): per 128-individual stage, three 2-D tiled loads
-//               (no multicast) into a 6-deep raw ring: the i-tile's and j-tile's one-hot
-//               genotype bytes (40 and 14 rows x 128 B) and the trait's 7 digit rows,
-//               128-byte swizzled; completion by mbarrier transaction bytes
-//   warps 0-3   A producers: one TMEM lane each; expand the raw i rows into the stage's A
-//               rows and store them into TMEM with tcgen05.st (the MMA reads A from TMEM)
-//   warps 4-7   B producers: expand raw j rows x digits into the stage's B tile (K-major,
-//               128-byte swizzle) in smem
-//   warps 8-11  epilogue: tcgen05.ld of the accumulator, lane-triplet shuffles, FP64
-//               statistics, warp-aggregated hit append, per-trait max F
-//   warp 12     TMEM allocator and MMA issuer (one thread): 4 x tcgen05.mma per stage
-// TMEM (512 columns): accumulators at [0, 224) and [224, 448), two A stages of 128
-// individuals (32 columns) at [448, 512). An M = 128, K = 32 int8 MMA takes nearly the same
-// time for any N from 192 to 256, so one wide instruction carries every column type; the j
-// tile is 14 SNPs so that two accumulators and two A stages fit the TMEM. 4-stage B ring,
-// 2-stage A ring, 2 accumulators, so the epilogue of one tile overlaps the MMAs of the next.
-// All waits are bounded (tc_ptx.cuh); a timeout sets counters[2] and every role leaves its
-// loop.
+//   warp 13       TMA loader (one thread): per 128-individual stage, the A stage (four 2-D
+//                 tiled loads of 30 h3 rows, into rows 32w..32w+29) and the raw stage (the
+//                 j-tile's 16 one-hot rows and the trait's 7 digit rows); no multicast;
+//                 completion by mbarrier transaction bytes
+//   warps 4-7     B producers: raw j rows x digits -> the stage's B tile (K-major, 128-byte
+//                 swizzle) in smem
+//   warp 12       TMEM allocator and MMA issuer (one thread): 4 x tcgen05.mma (A and B from
+//                 shared memory, N = 240) per stage
+//   warps 0-3, 8-11  epilogue, two warps per TMEM lane quarter, each taking three of the six
+//                 j rounds: tcgen05.ld of the accumulator, lane-triplet shuffles, FP64
+//                 statistics, warp-aggregated hit append, per-trait max F
+// TMEM (512 columns): accumulators at [0, 240) and [240, 480), so the epilogue of one tile
+// overlaps the MMAs of the next. All waits are bounded (tc_ptx.cuh); a timeout sets
+// counters[2] and every role leaves its loop.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -53,36 +53,38 @@
 namespace epi {
 namespace mma {
 
-constexpr int TI = 40;         // i-SNPs per tile (4 warps x 10 lane triplets)
-constexpr int TJ = 14;         // j-SNPs per tile
+constexpr int TI = 40;         // i-SNPs per tile (4 lane quarters x 10 triplets)
+constexpr int TJ = 16;         // j-SNPs per tile
 constexpr int NTY = 12;        // B column types per j-SNP: b (3) x {w, d0, d1, d2} ...
 constexpr int NTYPE = 15;      // ... and missing x {e0, e1, e2}
-constexpr int NCOL = TJ * NTYPE;           // 210 columns in use
-constexpr int N = (NCOL + 15) / 16 * 16;  // 224: MMA width (padding columns are zero)
+constexpr int N = TJ * NTYPE;  // 240
 constexpr int M = 128;
 constexpr int KS = 128;        // individuals per pipeline stage
 constexpr int STAGES = 4;      // B ring (smem)
-constexpr int ASTAGES = 2;     // A ring (TMEM)
+constexpr int ASTAGES = 4;     // A ring (smem, TMA)
+constexpr int RSTAGES = 6;     // raw ring (smem, TMA)
 constexpr int ND = 7;          // digit rows per trait: w, Y digits (3), E digits (3)
-constexpr uint32_t ACC_COL1 = N, A_COL = 2 * N;
+constexpr int ROUNDS = (TJ + 2) / 3;  // j rounds of the epilogue (3 j-SNPs per round)
+constexpr uint32_t ACC_COL1 = N;
 __host__ __device__ constexpr uint32_t acc_col(uint32_t buf) { return buf ? ACC_COL1 : 0u; }
-__host__ __device__ constexpr uint32_t a_col(uint32_t s) { return A_COL + 32 * s; }
 constexpr uint32_t TMEM_COLS = 512;
-constexpr int B_STAGE = N * KS;  // bytes per B stage (30 KB)
-constexpr int RSTAGES = 6;       // raw (TMA) ring depth
-// raw stage: one-hot genotype rows (40 i, 16 j) and the trait's digit rows
-constexpr int RAW_I = 0, RAW_J = TI * KS, RAW_D = RAW_J + 16 * KS;  // 1024-aligned sections
-constexpr int RAW_STAGE = 8 * 1024;
-constexpr uint32_t RAW_BYTES = (TI + TJ + ND) * KS;  // transaction bytes per raw stage
+constexpr int A_STAGE = M * KS;  // 16 KB
+constexpr int B_STAGE = N * KS;  // 30 KB
+constexpr int A_BOX = 30;        // h3 rows per TMA box (10 i-SNPs x 3 genotypes)
+constexpr uint32_t A_BYTES = 4 * A_BOX * KS;  // transaction bytes per A stage
+// raw stage: the j-tile's one-hot rows and the trait's digit rows, 1024-aligned sections
+constexpr int RAW_J = 0, RAW_D = TJ * KS;
+constexpr int RAW_STAGE = 4 * 1024;
+constexpr uint32_t RAW_BYTES = (TJ + ND) * KS;
 constexpr int NWARPS = 14;
 constexpr int NTHREADS = NWARPS * 32;
 constexpr uint32_t IDESC = tc::idesc_i8(M, N);
-static_assert(RAW_J % 1024 == 0 && RAW_D % 1024 == 0 && RAW_J + TJ * KS <= RAW_D && RAW_D + ND * KS <= RAW_STAGE,
-              "raw layout");
-static_assert(B_STAGE % 1024 == 0 && N % 16 == 0 && N <= 256, "B tile");
-static_assert(a_col(ASTAGES - 1) + KS / 4 <= TMEM_COLS, "TMEM layout");
+static_assert(RAW_D % 1024 == 0 && RAW_D + ND * KS <= RAW_STAGE, "raw layout");
+static_assert(B_STAGE % 1024 == 0 && A_STAGE % 1024 == 0 && N % 16 == 0 && N <= 256, "operand tiles");
+static_assert(2 * N <= (int)TMEM_COLS && ROUNDS % 2 == 0, "TMEM layout / epilogue split");
 
 struct Smem {
+    uint8_t a[ASTAGES][A_STAGE];
     uint8_t b[STAGES][B_STAGE];
     uint8_t raw[RSTAGES][RAW_STAGE];
     uint64_t full[STAGES], empty[STAGES], afull[ASTAGES], aempty[ASTAGES], raw_full[RSTAGES], raw_empty[RSTAGES],
@@ -207,7 +209,7 @@ __device__ __forceinline__ void advance(uint32_t &slot, uint32_t &phase)
 __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __grid_constant__ MmaMaps maps)
 {
     extern __shared__ uint8_t smem_raw[];
-    // the B stages need 1024-byte alignment (128-byte swizzle atoms)
+    // the operand stages need 1024-byte alignment (128-byte swizzle atoms)
     const uint32_t raw_s = tc::smem_u32(smem_raw);
     Smem &sm = *reinterpret_cast<Smem *>(smem_raw + (((raw_s + 1023u) & ~1023u) - raw_s));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -218,12 +220,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         tc::tmem_alloc(&sm.tmem_base, TMEM_COLS);
         tc::tmem_relinquish();
     }
-    // the B padding rows (columns NCOL..N-1 of every stage) are never written by the producers
-    for (int w = threadIdx.x; w < STAGES * (N - NCOL) * 8; w += blockDim.x) {
-        const int st = w / ((N - NCOL) * 8), n = NCOL + (w / 8) % (N - NCOL), c = w % 8;
-        *reinterpret_cast<uint4 *>(sm.b[st] + (n >> 3) * 1024 + (n & 7) * 128 + c * 16) = make_uint4(0, 0, 0, 0);
-    }
-    tc::fence_proxy_async_smem();
     // per-CTA maxima of F and F2 per trait (flushed to global memory once, at the end)
     unsigned int *smax = reinterpret_cast<unsigned int *>(reinterpret_cast<uint8_t *>(&sm) + sizeof(Smem));
     for (int w = threadIdx.x; w < 2 * a.ntraits; w += blockDim.x) smax[w] = 0u;
@@ -233,16 +229,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             tc::mbar_init(&sm.empty[s], 1);
         }
         for (int s = 0; s < ASTAGES; ++s) {
-            tc::mbar_init(&sm.afull[s], 4);
+            tc::mbar_init(&sm.afull[s], 1);
             tc::mbar_init(&sm.aempty[s], 1);
         }
         for (int r = 0; r < RSTAGES; ++r) {
             tc::mbar_init(&sm.raw_full[r], 1);
-            tc::mbar_init(&sm.raw_empty[r], 8);
+            tc::mbar_init(&sm.raw_empty[r], 4);
         }
         for (int b = 0; b < 2; ++b) {
             tc::mbar_init(&sm.acc_full[b], 1);
-            tc::mbar_init(&sm.acc_empty[b], 4);
+            tc::mbar_init(&sm.acc_empty[b], 8);
         }
         tc::mbar_init(&sm.drain, 1);
         sm.abort = 0;
@@ -254,50 +250,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
     const uint32_t tmem = sm.tmem_base;
     volatile int *abort = &sm.abort;
 
-    if (warp < 4) {
-        // ---------------- A producers: TMEM lane = threadIdx.x ----------------
-        const int ii = 10 * warp + lane / 3, ga = lane % 3;
-        const bool rowok = lane < 30;
-        const uint32_t taddr_lane = tmem + ((uint32_t)(32 * warp) << 16);
-        uint32_t as = 0, aph = 0, rs = 0, rph = 0;
-        bool ok = true;
-        for (long long u = blockIdx.x; u < units && ok; u += gridDim.x) {
-            const Unit un = decode(a, u);
-            if (un.skip) continue;
-            for (int ks = 0; ks < nks && ok; ++ks) {
-                if (!tc::mbar_wait(&sm.raw_full[rs], rph, abort)) {
-                    fail(a, sm, 1);
-                    ok = false;
-                    break;
-                }
-                uint32_t v[32];
-                const uint8_t *ri = sm.raw[rs] + RAW_I;
-#pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    const uint4 h = rowok ? ld_sw128(ri, ii, c) : make_uint4(0, 0, 0, 0);
-                    v[4 * c + 0] = (h.x >> ga) & 0x01010101u;
-                    v[4 * c + 1] = (h.y >> ga) & 0x01010101u;
-                    v[4 * c + 2] = (h.z >> ga) & 0x01010101u;
-                    v[4 * c + 3] = (h.w >> ga) & 0x01010101u;
-                }
-                if (!tc::mbar_wait(&sm.aempty[as], aph ^ 1u, abort)) {
-                    fail(a, sm, 1);
-                    ok = false;
-                    break;
-                }
-                tc::tmem_st32(taddr_lane + a_col(as), v);
-                // the raw slot is released after the store, which consumes every loaded value
-                __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&sm.raw_empty[rs]);
-                advance<RSTAGES>(rs, rph);
-                tc::tmem_wait_st();
-                tc::tc_fence_before();
-                __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&sm.afull[as]);
-                advance<ASTAGES>(as, aph);
-            }
-        }
-    } else if (warp < 8) {
+    if (warp >= 4 && warp < 8) {
         // ---------------- B producers: thread -> (j-SNP, 16-individual chunk) ----------------
         const int t = threadIdx.x - 128, jj = t >> 3, c = t & 7;
         uint32_t stage = 0, phase = 0, rs = 0, rph = 0;
@@ -312,14 +265,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     break;
                 }
                 const uint8_t *raw = sm.raw[rs];
-                const bool jok = jj < TJ;  // threads 112-127 have no j row
-                const uint4 h = jok ? ld_sw128(raw + RAW_J, jj, c) : make_uint4(0, 0, 0, 0);
+                const uint4 h = ld_sw128(raw + RAW_J, jj, c);
                 uint4 d[ND];
 #pragma unroll
                 for (int s2 = 0; s2 < ND; ++s2) d[s2] = ld_sw128(raw + RAW_D, s2, c);
                 uint8_t *base = sm.b[stage];
                 auto put = [&](int ty, const uint4 &m, const uint4 &dv) {
-                    if (!jok) return;
                     const int n = ty * TJ + jj;
                     uint4 o;
                     o.x = m.x & dv.x;
@@ -361,8 +312,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             }
         }
     } else if (warp < 12) {
-        // ---------------- epilogue ----------------
-        const int e = warp - 8;
+        // ---------------- epilogue: warps 0-3 rounds 0-2, warps 8-11 rounds 3-5 ----------------
+        const int e = warp & 3, rho0 = warp < 4 ? 0 : ROUNDS / 2;
         const int ii = 10 * e + lane / 3, ga = lane % 3, tbase = (lane / 3) * 3;
         const bool rowok = lane < 30;
         const uint32_t tl = tmem + ((uint32_t)(32 * e) << 16);
@@ -386,7 +337,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             const uint32_t acc = tl + acc_col(buf);
             const bool report = a.report_trait < 0 || a.report_trait == t;
 #pragma unroll 1
-            for (int rho = 0; rho < (TJ + 2) / 3; ++rho) {
+            for (int rho = rho0; rho < rho0 + ROUNDS / 2; ++rho) {
                 const int jb = 3 * rho;
                 const int jl = jb + ga;
                 const int dj = un.j0 + jl;
@@ -469,12 +420,24 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
     } else if (warp == 13) {
         // ---------------- TMA loader ----------------
         if (lane == 0) {
-            uint32_t rs = 0, rph = 0, issued = 0;
+            uint32_t as = 0, aph = 0, rs = 0, rph = 0, issued_a = 0, issued_r = 0;
             bool ok = true;
             for (long long u = blockIdx.x; u < units && ok; u += gridDim.x) {
                 const Unit un = decode(a, u);
                 if (un.skip) continue;
+                const int arow = 3 * (un.bd.start1 + un.i0);
                 for (int ks = 0; ks < nks; ++ks) {
+                    if (!tc::mbar_wait(&sm.aempty[as], aph ^ 1u, abort)) {
+                        fail(a, sm, 7);
+                        ok = false;
+                        break;
+                    }
+                    tc::mbar_arrive_expect_tx(&sm.afull[as], A_BYTES);
+#pragma unroll
+                    for (int w = 0; w < 4; ++w)
+                        tc::tma_load_2d(sm.a[as] + 32 * w * KS, &maps.hi, ks * KS, arow + A_BOX * w, &sm.afull[as]);
+                    ++issued_a;
+                    advance<ASTAGES>(as, aph);
                     if (!tc::mbar_wait(&sm.raw_empty[rs], rph ^ 1u, abort)) {
                         fail(a, sm, 7);
                         ok = false;
@@ -482,26 +445,28 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     }
                     uint8_t *raw = sm.raw[rs];
                     tc::mbar_arrive_expect_tx(&sm.raw_full[rs], RAW_BYTES);
-                    tc::tma_load_2d(raw + RAW_I, &maps.hi, ks * KS, un.bd.start1 + un.i0, &sm.raw_full[rs]);
                     tc::tma_load_2d(raw + RAW_J, &maps.hj, ks * KS, un.bd.start2 + un.j0, &sm.raw_full[rs]);
                     tc::tma_load_2d(raw + RAW_D, &maps.dg, ks * KS, ND * un.trait, &sm.raw_full[rs]);
-                    ++issued;
+                    ++issued_r;
                     advance<RSTAGES>(rs, rph);
                 }
             }
             // no TMA write may still be landing in shared memory when the CTA exits: wait for
-            // the last load issued into every ring slot (already complete on the normal path)
+            // the last load issued into every ring slot (already complete on the normal path).
+            // The load issued `back` loads ago went to slot (next - back) and completes the
+            // parity of the current lap, or of the previous one when it wrapped.
             int no_abort = 0;
-            for (uint32_t k = 0; k < RSTAGES && k < issued; ++k) {
-                // the slot used k+1 loads ago, and the parity its load completes
-                const uint32_t back = k + 1;
-                const uint32_t slot = (rs + RSTAGES - (back % RSTAGES)) % RSTAGES;
-                const uint32_t par = (back > rs) ? (rph ^ 1u) : rph;
+            for (uint32_t back = 1; back <= ASTAGES && back <= issued_a; ++back) {
+                const uint32_t slot = (as + ASTAGES - back) % ASTAGES, par = back > as ? (aph ^ 1u) : aph;
+                if (!tc::mbar_wait(&sm.afull[slot], par, &no_abort)) fail(a, sm, 8);
+            }
+            for (uint32_t back = 1; back <= RSTAGES && back <= issued_r; ++back) {
+                const uint32_t slot = (rs + RSTAGES - back) % RSTAGES, par = back > rs ? (rph ^ 1u) : rph;
                 if (!tc::mbar_wait(&sm.raw_full[slot], par, &no_abort)) fail(a, sm, 8);
             }
         }
     } else if (lane == 0) {
-        // ---------------- MMA issuer ----------------
+        // ---------------- MMA issuer (warp 12) ----------------
         uint32_t stage = 0, phase = 0, as = 0, aph = 0, accph[2] = {0u, 0u};
         int buf = 0;
         bool ok = true;
@@ -521,10 +486,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     break;
                 }
                 tc::tc_fence_after();
-                const uint32_t bs = tc::smem_u32(sm.b[stage]);
+                const uint32_t asb = tc::smem_u32(sm.a[as]), bsb = tc::smem_u32(sm.b[stage]);
 #pragma unroll
                 for (int kk = 0; kk < KS / 32; ++kk)
-                    tc::mma_i8_ts(d, tmem + a_col(as) + 8 * kk, tc::smem_desc_sw128(bs + 32 * kk), IDESC,
+                    tc::mma_i8_ss(d, tc::smem_desc_sw128(asb + 32 * kk), tc::smem_desc_sw128(bsb + 32 * kk), IDESC,
                                   (ks | kk) != 0);
                 tc::mma_commit(&sm.empty[stage]);
                 tc::mma_commit(&sm.aempty[as]);
@@ -537,7 +502,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             buf ^= 1;
         }
         // every MMA issued above has completed once `drain` flips (waited for even after an
-        // abort: the accumulators and A stages must be idle before the TMEM is released)
+        // abort: the accumulators must be idle before the TMEM is released)
         tc::mma_commit(&sm.drain);
         int no_abort = 0;
         if (!tc::mbar_wait(&sm.drain, 0, &no_abort)) fail(a, sm, 6);
@@ -555,9 +520,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
 
 }  // namespace mma
 
-// Tensor maps of the tensor form's TMA loads: the one-hot genotype bytes [nsnp][Np] with
-// boxes of 40 and 16 rows x 128 bytes, and the trait digit rows [7T][Np] with 7-row boxes;
-// all 128-byte swizzled, out-of-range rows read as zero.
+// Tensor maps of the tensor form's TMA loads: the genotype-indicator rows h3 [3 nsnp][Np]
+// with 30-row boxes (A), the one-hot genotype bytes [nsnp][Np] with 16-row boxes (j side) and
+// the trait digit rows [7T][Np] with 7-row boxes; all 128 bytes wide, 128-byte swizzled,
+// out-of-range rows read as zero.
 static cudaError_t encode_2d(CUtensorMap *m, const void *base, uint64_t inner, uint64_t rows, uint32_t box_rows)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -578,9 +544,9 @@ static cudaError_t encode_2d(CUtensorMap *m, const void *base, uint64_t inner, u
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-cudaError_t mma_encode_genotypes(MmaMaps *maps, const uint8_t *hcodes, int nsnp, int Np)
+cudaError_t mma_encode_genotypes(MmaMaps *maps, const uint8_t *hcodes, const uint8_t *h3, int nsnp, int Np)
 {
-    cudaError_t e = encode_2d(&maps->hi, hcodes, (uint64_t)Np, (uint64_t)nsnp, mma::TI);
+    cudaError_t e = encode_2d(&maps->hi, h3, (uint64_t)Np, 3 * (uint64_t)nsnp, mma::A_BOX);
     if (e == cudaSuccess) e = encode_2d(&maps->hj, hcodes, (uint64_t)Np, (uint64_t)nsnp, mma::TJ);
     return e;
 }
