@@ -232,6 +232,14 @@ __device__ __forceinline__ void emit_row(const ScanArgs &a, bool hit, int snp1, 
 }
 
 // Warp max of F (NaN ignored) folded into the per-trait maximum. Every lane calls it.
+// Warp maximum of already-encoded values, one atomicMax on `slot` (every lane must call it).
+__device__ __forceinline__ void fold_max_enc(unsigned int *slot, unsigned int v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31u) == 0u && v) atomicMax(slot, v);
+}
+
 __device__ __forceinline__ void fold_max(unsigned int *slot, bool valid, double F)
 {
     unsigned int v = (valid && F == F) ? f2ord((float)F) : 0u;

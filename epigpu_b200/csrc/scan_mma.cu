@@ -139,10 +139,18 @@ __device__ __forceinline__ double rcp_d(double x)
     return fma(r, e, r);
 }
 
+// num / den in FP64: by rcp_d when den is a normal single-precision magnitude (relative error
+// ~2^-46), else by IEEE division (zero, tiny or huge denominators keep division's inf / NaN).
+__device__ __forceinline__ double div_fast(double num, double den)
+{
+    const double ad = fabs(den);
+    return (ad > 1e-30 && ad < 1e30) ? num * rcp_d(den) : num / den;
+}
+
 // The reference's 8 df / 4 df statistics (src/EpiOpenCL.c:231-247, :452-486) in FP64 from
 // the exact integer cell counts n and digit sums si (S = si * sc), and Q = sum of y^2 over
 // the pair's valid individuals. Same quantities as pair_stat, arranged to avoid division
-// chains: reciprocals of counts by rcp_d, one IEEE division for F and one for F2.
+// chains: reciprocals by rcp_d.
 __device__ __forceinline__ PairStat pair_stat_exact(const int n[9], const long long si[9], double sc, double Q,
                                                     bool want_int)
 {
@@ -171,7 +179,7 @@ __device__ __forceinline__ PairStat pair_stat_exact(const int n[9], const long l
     r.nfac = nfac;
     r.d1 = nfac - 1;
     r.d2 = N - nfac;
-    r.F = (SSB * (double)r.d2) / (SSW * (double)r.d1);
+    r.F = div_fast(SSB * (double)r.d2, SSW * (double)r.d1);
     r.F2 = 0.0;
     if (want_int) {
         double row[3], col[3];
@@ -192,7 +200,7 @@ __device__ __forceinline__ PairStat pair_stat_exact(const int n[9], const long l
                 SSI = fma((double)n[c] * t, t, SSI);
             }
         }
-        r.F2 = (SSI * (double)r.d2) / (4.0 * SSW);
+        r.F2 = div_fast(SSI * (double)r.d2, 4.0 * SSW);
     }
     return r;
 }
@@ -336,6 +344,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             tc::tc_fence_after();
             const uint32_t acc = tl + acc_col(buf);
             const bool report = a.report_trait < 0 || a.report_trait == t;
+            unsigned int fmx = 0u, f2mx = 0u;  // this thread's largest F, F2 of the tile (encoded)
 #pragma unroll 1
             for (int rho = rho0; rho < rho0 + ROUNDS / 2; ++rho) {
                 const int jb = 3 * rho;
@@ -408,9 +417,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 }
                 const bool hit = valid && report && is_hit(a, s);
                 emit_hit(a, hit, un.bd.start1 + di, un.bd.start2 + dj, s, t, un.block);
-                fold_max(&smax[t], valid, s.F);
-                if (a.test_int) fold_max(&smax[a.ntraits + t], valid, s.F2);
+                if (valid && s.F == s.F) fmx = max(fmx, f2ord((float)s.F));
+                if (valid && s.F2 == s.F2) f2mx = max(f2mx, f2ord((float)s.F2));
             }
+            fold_max_enc(&smax[t], fmx);
+            if (a.test_int) fold_max_enc(&smax[a.ntraits + t], f2mx);
             tc::tc_fence_before();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&sm.acc_empty[buf]);
