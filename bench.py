@@ -37,6 +37,8 @@ WORKLOADS = {
     "cfg5": (8000, None, "f", 8, "8 df scan, N=8,000, 22 uneven blocks (M=250,000), 8 traits with own masks"),
     # the cfg3 kernel on a block small enough for an ncu capture of one launch
     "cfg3s": (10000, [4000], "i", 1, "8 df + 4 df scan, N=10,000 individuals, M=4,000 SNPs (profiling size)"),
+    # the cfg3 kernel with operands larger than L2 (DRAM traffic per pair as in cfg3)
+    "cfg3m": (10000, [20000], "i", 1, "8 df + 4 df scan, N=10,000 individuals, M=20,000 SNPs (traffic capture)"),
 }
 
 
@@ -403,8 +405,15 @@ def main():
             # digits} + 3 y^2 digits) per individual; the 128 x 240 tile carries 48 (padding rows)
             ops_pair = 2.0 * 45.0 * nid
             achieved = pairs_launch * ops_pair / kern_s / 1e12
+            # DRAM bytes per launch: the ncu capture of the same kernel on the cfg3m workload
+            # (N=10,000, M=20,000, operands larger than L2) read 13.178 GB for 199,990,000
+            # pairs over Np = 10,112 padded individuals; the j rows are streamed once per i
+            # tile, so the bytes scale with pairs x Np (profiles/scan_mma_traffic_cfg3m.md)
+            np_pad = (nid + 127) // 128 * 128
+            traffic = 13.178e9 / (199990000.0 * 10112.0) * pairs_launch * np_pad
             roof = {"bound": "tensor", "achieved": achieved, "peak": int8, "unit": "TOP/s",
-                    "frac": achieved / int8, "traffic": None,
+                    "frac": achieved / int8, "traffic": traffic, "traffic_unit": "bytes per launch",
+                    "traffic_source": "ncu dram__bytes_read+write on cfg3m, scaled by pairs x individuals",
                     "peak_source": "cuBLAS int8 GEMM measured in this run (torch._int_mm 8192^3)"}
         else:
             # plain form: 10 FP32 FMAs per pair and individual (9 cell sums + sum of squares)
@@ -438,7 +447,8 @@ def main():
         }
         if popc:
             out["popc_form"] = popc
-            out["tensor_over_popc"] = value / world / popc["value"]
+            # kernel time against kernel time (the popcount sample is timed by kernel events)
+            out["tensor_over_popc"] = pairs_step / (statistics.mean(kernel_ms) / 1e3) / popc["value"]
         print(json.dumps(out))
     ctx.close()
     if pg:
