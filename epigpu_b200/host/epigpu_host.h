@@ -44,6 +44,7 @@ extern int UCHUNKSIZE;
 extern int UTEST;
 extern int USAFE;
 extern int UFORM;
+extern int UNPERM; /* -N: permutations scanned beside the phenotype (0 = none) */
 extern char plinkbin[100];
 extern float UTHRESHOLD1, UTHRESHOLD2;
 extern char UPHEN[1000];
@@ -62,6 +63,10 @@ int write_epigpu(const char *filename, const epigpu_data *d);
 void free_epigpu(epigpu_data *d);
 int read_phenotype_file(const char *filename, int nid, ped *dat);
 int is_binary_phenotype(int nid, const ped *dat);
+
+/* plink.c: data mode */
+int plink_to_epigpu(const char *pedfile, const char *mapfile, const char *binfile, char *err, size_t errlen);
+int epigpu_to_plink(const char *binfile, const char *pedfile, const char *mapfile, char *err, size_t errlen);
 
 /* scan_driver.c */
 int perform_scan(int *geno, chromosome *chrstat, ped *dat, map *genmap, int nid, int nsnp, int npack, int remain,

@@ -22,12 +22,16 @@ int UCHUNKSIZE = 128;
 int UTEST = 'f';
 int USAFE = 0;
 int UFORM = EPI_FORM_AUTO;
+int UNPERM = 0;
 char plinkbin[100];
 float UTHRESHOLD1 = 6.5f, UTHRESHOLD2 = 10.5f;
 char UPHEN[1000];
 
 static const char *usage_text =
     "\n\nepiGPU (B200) performs an exhaustive 2D scan for epistasis\n\n"
+    "DATA MODE:\n\n"
+    "<epigpu> -Dr [ .ped file ] [ .map file ] [ epigpu file ]\tread PLINK data into an epigpu file\n"
+    "<epigpu> -De [ .ped file ] [ .map file ] [ epigpu file ]\textract an epigpu file to PLINK data\n\n"
     "ANALYSIS MODE:\n\n"
     "<epigpu> -A [ epigpu file] [ output file] [ Options ... ]\n\n"
     "Options:\n\n"
@@ -39,7 +43,9 @@ static const char *usage_text =
     "I [n]\tF value threshold for interaction test, default [n] = 10.5\n"
     "s [0/1]\tNormal / Safe mode. Default = 0 (Normal mode)\n"
     "P [file]\tSeparate phenotype file, one value per individual\n"
-    "g [a/p/t]\tGPU form: automatic, plain popcount, tensor core. Default = a\n\n"
+    "g [a/p/t]\tGPU form: automatic, plain popcount, tensor core. Default = a\n"
+    "N [n]\tPermutation threshold: also scan n permutations of the phenotype in the same launches\n"
+    "\tand write each one's largest F and the family-wise thresholds to <output file>.perm\n\n"
     "Example:\n"
     "<epigpu> -A [ epigpu file ] [ output file ]\n"
     "<epigpu> -A [ epigpu file ] [ output file ] -i 512 -p 100 -F 7\n\n\n";
@@ -148,6 +154,14 @@ static void parse_analysis_args(int argc, char **argv, char **binfile, char **ou
             snprintf(UPHEN, sizeof(UPHEN), "%s", v);
             break;
         }
+        case 'N':
+            UNPERM = atoi(v);
+            if (UNPERM < 0 || UNPERM > 100000) {
+                printf("Permutation threshold: the number of phenotype permutations scanned with the data, "
+                       "0 to 100000\nDefault = 0 (none)\n\n");
+                exit(1);
+            }
+            break;
         case 'g':
             if (v[0] == 'a') UFORM = EPI_FORM_AUTO;
             else if (v[0] == 'p') UFORM = EPI_FORM_POPC;
@@ -183,6 +197,44 @@ static void permute_records(int nid, ped *dat)
     }
 }
 
+/* Data mode (src/readplink.c:1296-1431): -Dr reads a PLINK .ped/.map fileset into a .epigpu
+ * file, -De writes one back out as text. The reference's other data-mode letters (c clean,
+ * m impute, n random phenotype, s/q simulate, g GenABEL, u unpacked) are data preparation
+ * outside the scan and are refused with a message. */
+static int data_mode(int argc, char **argv)
+{
+    const char *flags = argv[1] + 2;
+    int read = 0, extract = 0;
+    if (strlen(argv[1]) > 6) {
+        printf("Wrong flags\n%s", usage_text);
+        exit(1);
+    }
+    for (const char *c = flags; *c; ++c) {
+        if (*c == 'r') read = 1;
+        else if (*c == 'e') extract = 1;
+        else {
+            printf("Data mode letter '%c' (cleaning, imputation, simulation, GenABEL or unpacked output) is not part of "
+                   "this program; it reads PLINK data (-Dr) and extracts it (-De).\n", *c);
+            exit(1);
+        }
+    }
+    if (read == extract || argc != 5) {
+        printf("Wrong arguments\n%s", usage_text);
+        exit(1);
+    }
+    char err[512];
+    int rc;
+    if (extract)
+        rc = epigpu_to_plink(argv[4], argv[2], argv[3], err, sizeof(err));
+    else
+        rc = plink_to_epigpu(argv[2], argv[3], argv[4], err, sizeof(err));
+    if (rc) {
+        printf("\n%s\n", err);
+        exit(1);
+    }
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
     if (argc < 3) {
@@ -193,11 +245,7 @@ int main(int argc, char **argv)
         printf("Incorrect arguments\n%s", usage_text);
         exit(1);
     }
-    if (argv[1][1] == 'D') {
-        printf("Data mode (-D) is not part of this program: write .epigpu files with epiGPU's data mode or "
-               "epigpu_b200.epigpu_file.\n");
-        exit(1);
-    }
+    if (argv[1][1] == 'D') return data_mode(argc, argv);
     if (argv[1][1] != 'A') {
         printf("%s", usage_text);
         exit(1);

@@ -22,6 +22,7 @@
  *    partial rows;
  *  - errors print the library's message and exit with its status (ereport, :1159-1177).
  */
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -140,6 +141,69 @@ static void write_header_full(const char *filename, int nid, int nsnp)
     fclose(out);
 }
 
+static int cmp_float(const void *a, const void *b)
+{
+    const float x = *(const float *)a, y = *(const float *)b;
+    return (x > y) - (x < y);
+}
+
+/* Empirical family-wise threshold at level alpha: the ceil((1 - alpha) K)-th smallest of the
+ * K permutation maxima (sorted ascending). */
+static float fw_threshold(const float *sorted, int K, double alpha)
+{
+    int k = (int)ceil((1.0 - alpha) * K);
+    if (k < 1) k = 1;
+    if (k > K) k = K;
+    return sorted[k - 1];
+}
+
+/* <filename>.perm: the largest F (and F2) over all pairs of every permuted phenotype, the
+ * family-wise thresholds they give, and the family-wise p-value of the observed largest F. */
+static void write_permutation_summary(const char *filename, int ntraits, const float *maxf, const float *maxf2)
+{
+    const int K = ntraits - 1;
+    char fn[1200];
+    snprintf(fn, sizeof(fn), "%s.perm", filename);
+    FILE *f = fopen(fn, "w");
+    if (!f) {
+        printf("Cannot write %s\n", fn);
+        exit(1);
+    }
+    float *s1 = (float *)malloc(sizeof(float) * (size_t)K), *s2 = (float *)malloc(sizeof(float) * (size_t)K);
+    int above = 0, above2 = 0;
+    for (int p = 0; p < K; p++) {
+        s1[p] = maxf[p + 1];
+        s2[p] = maxf2[p + 1];
+        above += s1[p] >= maxf[0];
+        above2 += s2[p] >= maxf2[0];
+    }
+    qsort(s1, (size_t)K, sizeof(float), cmp_float);
+    qsort(s2, (size_t)K, sizeof(float), cmp_float);
+    const int inter = UTEST == 'i';
+    fprintf(f, "Datafile: %s %s\n", plinkbin, UPHEN);
+    fprintf(f, "Permutations: %d (phenotype shuffled as by -p p, p = 1..%d)\n", K, K);
+    fprintf(f, "Test: %s\n", inter ? "interactions + full" : "full");
+    fprintf(f, "Observed largest F: %f\n", maxf[0]);
+    fprintf(f, "Family-wise p-value of the observed largest F: %f\n", (1.0 + above) / (K + 1.0));
+    fprintf(f, "Family-wise 5%% threshold for F: %f\n", fw_threshold(s1, K, 0.05));
+    fprintf(f, "Family-wise 1%% threshold for F: %f\n", fw_threshold(s1, K, 0.01));
+    if (inter) {
+        fprintf(f, "Observed largest Fint: %f\n", maxf2[0]);
+        fprintf(f, "Family-wise p-value of the observed largest Fint: %f\n", (1.0 + above2) / (K + 1.0));
+        fprintf(f, "Family-wise 5%% threshold for Fint: %f\n", fw_threshold(s2, K, 0.05));
+        fprintf(f, "Family-wise 1%% threshold for Fint: %f\n", fw_threshold(s2, K, 0.01));
+    }
+    fprintf(f, "\nPerm\tmaxF%s\n", inter ? "\tmaxFint" : "");
+    for (int p = 1; p <= K; p++) {
+        if (inter) fprintf(f, "%d\t%f\t%f\n", p, maxf[p], maxf2[p]);
+        else fprintf(f, "%d\t%f\n", p, maxf[p]);
+    }
+    fclose(f);
+    free(s1);
+    free(s2);
+    printf("Permutation maxima and family-wise thresholds written to %s\n", fn);
+}
+
 int perform_scan(int *geno, chromosome *chrstat, ped *dat, map *genmap, int nid, int nsnp, int npack, int remain,
                  int nchr, char *filename)
 {
@@ -168,6 +232,11 @@ int perform_scan(int *geno, chromosome *chrstat, ped *dat, map *genmap, int nid,
                    "filename.\n");
             exit(1);
         }
+        if (UNPERM > 0) {
+            printf("A permutation threshold (-N) needs every block scanned in one run; %s already holds part of "
+                   "a scan. Please use a different filename.\n", filename);
+            exit(1);
+        }
         printf("Resuming from %d/%d, %d hits found so far...\n\n", ccount + 1, chrint, tothits);
     } else {
         write_header_full(filename, nid, nsnp);
@@ -175,11 +244,32 @@ int perform_scan(int *geno, chromosome *chrstat, ped *dat, map *genmap, int nid,
 
     st = epi_load_packed(ctx, (const int32_t *)geno, nid, nsnp, npack, remain);
     if (st != EPI_OK) fail(ctx, st, "loading genotypes");
-    float *phen = (float *)malloc(sizeof(float) * (size_t)nid);
+    /* trait 0 is the phenotype; with -N, traits 1..UNPERM are its permutations p = 1..UNPERM
+     * by the -p rule (src/main.c:336-357), scanned in the same launches */
+    const int ntraits = 1 + UNPERM;
+    float *phen = (float *)malloc(sizeof(float) * (size_t)nid * ntraits);
+    uint8_t *valid = (uint8_t *)malloc((size_t)nid * ntraits);
+    if (!phen || !valid) {
+        printf("Out of host memory for %d phenotype columns\n", ntraits);
+        exit(1);
+    }
     for (int i = 0; i < nid; i++) phen[i] = dat[i].phen;
-    st = epi_set_phenotype(ctx, phen, nid, USAFE);
+    for (int t = 1; t < ntraits; t++) {
+        memcpy(phen + (size_t)t * nid, phen, sizeof(float) * (size_t)nid);
+        epi_permute_phenotype(phen + (size_t)t * nid, nid, (uint32_t)t);
+    }
+    if (UNPERM == 0) {
+        st = epi_set_phenotype(ctx, phen, nid, USAFE);
+    } else {
+        for (size_t k = 0; k < (size_t)nid * ntraits; k++) valid[k] = USAFE ? 1 : (phen[k] != -9.0f);
+        st = epi_set_traits(ctx, phen, nid, ntraits, valid);
+    }
     if (st != EPI_OK) fail(ctx, st, "loading the phenotype");
     free(phen);
+    free(valid);
+    float *maxf = (float *)malloc(sizeof(float) * (size_t)ntraits * 4);
+    float *maxf2 = maxf + ntraits, *accf = maxf + 2 * ntraits, *accf2 = maxf + 3 * ntraits;
+    for (int t = 0; t < ntraits; t++) accf[t] = accf2[t] = -INFINITY;
 
     epi_scan_opts opts;
     epi_default_opts(&opts);
@@ -225,7 +315,7 @@ int perform_scan(int *geno, chromosome *chrstat, ped *dat, map *genmap, int nid,
             printf("%d/%d\tScanning %s vs %s\n", ++ccount, chrint, chrstat[bi[b]].chrname, chrstat[bj[b]].chrname);
         fflush(stdout);
         int64_t n = 0;
-        st = epi_scan(ctx, blocks + b0, b1 - b0, &opts, hits, cap, &n, hblock, NULL, NULL, NULL);
+        st = epi_scan(ctx, blocks + b0, b1 - b0, &opts, hits, cap, &n, hblock, NULL, maxf, maxf2);
         if (st == EPI_E_OVERFLOW) {
             free(hits);
             free(hblock);
@@ -236,9 +326,13 @@ int perform_scan(int *geno, chromosome *chrstat, ped *dat, map *genmap, int nid,
                 printf("Out of host memory for %lld results\n", (long long)n);
                 exit(1);
             }
-            st = epi_scan(ctx, blocks + b0, b1 - b0, &opts, hits, cap, &n, hblock, NULL, NULL, NULL);
+            st = epi_scan(ctx, blocks + b0, b1 - b0, &opts, hits, cap, &n, hblock, NULL, maxf, maxf2);
         }
         if (st != EPI_OK) fail(ctx, st, "scanning");
+        for (int t = 0; t < ntraits; t++) {
+            if (maxf[t] > accf[t]) accf[t] = maxf[t];
+            if (maxf2[t] > accf2[t]) accf2[t] = maxf2[t];
+        }
         double ms = 0.0;
         epi_last_timing(ctx, &ms, NULL, NULL, NULL);
         gpu_ms += ms;
@@ -275,6 +369,8 @@ int perform_scan(int *geno, chromosome *chrstat, ped *dat, map *genmap, int nid,
         printf("\n\t%d blocks scanned on the GPU in %s (%.3f s)\n\n", b1 - b0, tt, ms / 1000.0);
         b0 = b1;
     }
+    if (UNPERM > 0) write_permutation_summary(filename, ntraits, accf, accf2);
+    free(maxf);
     free(hits);
     free(hblock);
     free(blocks);

@@ -98,3 +98,75 @@ def test_resume_after_interruption(tmp_path):
     r = subprocess.run([str(CLI), "-A", str(path), str(full), *args], capture_output=True, text=True, timeout=300)
     assert "Scan already completed" in r.stdout
 
+
+
+def test_plink_fileset_to_scan(tmp_path):
+    """PLINK text in, results out: epiGPU -Dr turns a .ped/.map fileset into a .epigpu file
+    and epiGPU -A scans it (tensor form); the hits match the FP64 oracle run on the genotype
+    codes and phenotypes the file holds."""
+    import test_datamode
+    ped, mp = test_datamode.write_plink(tmp_path, 300, 150, seed=21)
+    path = tmp_path / "plink.epigpu"
+    r = subprocess.run([str(CLI), "-Dr", str(ped), str(mp), str(path)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    d = epigpu_file.read(path)
+    codes = oracles.oracle_unpack(d.gpack, d.nid)
+    phen = d.ped["phen"].astype(np.float32)
+    out = tmp_path / "res.txt"
+    t1 = float(np.float32(synth.f_threshold(8, d.nid - 9, 5e-2)))
+    t2 = float(np.float32(synth.f_threshold(4, d.nid - 9, 5e-2)))
+    r = subprocess.run([str(CLI), "-A", str(path), str(out), "-t", "i", "-F", "%.6f" % t1, "-I", "%.6f" % t2,
+                        "-g", "t"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    header, blocks = parse_results(out)
+    assert len(blocks) == d.nchr * (d.nchr + 1) // 2
+    total = 0
+    for (c1, c2, rows), blk in zip(blocks, d.blocks()):
+        got = np.array([(int(x[0]) - 1, int(x[3]) - 1) for x in rows], dtype=[("snp1", "i4"), ("snp2", "i4")])
+        hb, tb, pb = oracles.oracle_scan_block(codes, phen, blk, test="i", t1=t1, t2=t2, per_pair=True)
+        excl = parity.near_threshold(pb, blk, t1, t2, "i", 1e-4)
+        ok, msg = parity.compare_hit_lists(got, hb, excl)
+        assert ok, "block %d x %d: %s" % (c1, c2, msg)
+        total += len(rows)
+    assert total > 0
+
+
+def test_permutation_threshold(tmp_path):
+    """-N n scans n permuted phenotypes (the -p rule, p = 1..n) in the same launches: the
+    results file is the one a plain run writes, and <output>.perm holds each permutation's
+    largest F / Fint over every pair, which must match the FP64 oracle's maximum for that
+    permuted phenotype, with the family-wise thresholds and p-value computed from them."""
+    path, d, codes, phen = make_data(tmp_path, nid=300, sizes=(70, 50), seed=8)
+    K = 20
+    plain, perm = tmp_path / "plain.txt", tmp_path / "perm.txt"
+    args = ["-t", "i", "-F", "5.0", "-I", "6.0", "-g", "t"]
+    for out, extra in ((plain, []), (perm, ["-N", str(K)])):
+        r = subprocess.run([str(CLI), "-A", str(path), str(out), *args, *extra], capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+    assert plain.read_text() == perm.read_text()
+    lines = (tmp_path / "perm.txt.perm").read_text().splitlines()
+    head = dict(ln.split(": ", 1) for ln in lines if ": " in ln)
+    table = lines[lines.index("Perm\tmaxF\tmaxFint") + 1:]
+    assert len(table) == K
+    got = np.array([[float(x) for x in ln.split("\t")[1:]] for ln in table])
+
+    def max_stats(y):
+        mf = mf2 = -np.inf
+        for blk in d.blocks():
+            _, _, pb = oracles.oracle_scan_block(codes, y, blk, test="i", t1=1e30, t2=1e30, per_pair=True)
+            s1, m1, s2, m2 = blk
+            gx, gy = np.meshgrid(np.arange(m1), np.arange(m2), indexing="ij")
+            ok = (gx + s1 > gy + s2) & np.isfinite(pb["F"]) & (pb["df1"] > 0)
+            mf = max(mf, pb["F"][ok].max())
+            mf2 = max(mf2, pb["F2"][ok & np.isfinite(pb["F2"])].max())
+        return mf, mf2
+
+    obs = max_stats(phen)
+    assert abs(float(head["Observed largest F"]) - obs[0]) <= 1e-5 * obs[0] + 1e-6
+    want = np.array([max_stats(oracles.oracle_permute(phen, p)) for p in range(1, K + 1)])
+    assert np.all(np.abs(got - want) <= 1e-5 * np.abs(want) + 1e-6), np.abs(got - want).max()
+    srt = np.sort(got[:, 0])
+    assert abs(float(head["Family-wise 5% threshold for F"]) - srt[int(np.ceil(0.95 * K)) - 1]) <= 1e-5 * srt[-1]
+    pval = (1 + np.sum(got[:, 0] >= float(head["Observed largest F"]))) / (K + 1)
+    assert abs(float(head["Family-wise p-value of the observed largest F"]) - pval) < 1e-6
