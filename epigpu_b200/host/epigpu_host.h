@@ -44,6 +44,7 @@ extern int UCHUNKSIZE;
 extern int UTEST;
 extern int USAFE;
 extern int UFORM;
+extern int UREFRESUME; /* -R: resume with the reference's restart-column rule */
 extern int UNPERM; /* -N: permutations scanned beside the phenotype (0 = none) */
 extern char plinkbin[100];
 extern float UTHRESHOLD1, UTHRESHOLD2;

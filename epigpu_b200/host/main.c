@@ -23,6 +23,7 @@ int UTEST = 'f';
 int USAFE = 0;
 int UFORM = EPI_FORM_AUTO;
 int UNPERM = 0;
+int UREFRESUME = 0;
 char plinkbin[100];
 float UTHRESHOLD1 = 6.5f, UTHRESHOLD2 = 10.5f;
 char UPHEN[1000];
@@ -45,7 +46,9 @@ static const char *usage_text =
     "P [file]\tSeparate phenotype file, one value per individual\n"
     "g [a/p/t]\tGPU form: automatic, plain popcount, tensor core. Default = a\n"
     "N [n]\tPermutation threshold: also scan n permutations of the phenotype in the same launches\n"
-    "\tand write each one's largest F and the family-wise thresholds to <output file>.perm\n\n"
+    "\tand write each one's largest F and the family-wise thresholds to <output file>.perm\n"
+    "R [0/1]\tResume exactly as the reference does (1 also skips, on later chromosomes, the blocks\n"
+    "\tbefore the restart column). Default = 0\n\n"
     "Example:\n"
     "<epigpu> -A [ epigpu file ] [ output file ]\n"
     "<epigpu> -A [ epigpu file ] [ output file ] -i 512 -p 100 -F 7\n\n\n";
@@ -154,6 +157,9 @@ static void parse_analysis_args(int argc, char **argv, char **binfile, char **ou
             snprintf(UPHEN, sizeof(UPHEN), "%s", v);
             break;
         }
+        case 'R':
+            UREFRESUME = atoi(v) != 0;
+            break;
         case 'N':
             UNPERM = atoi(v);
             if (UNPERM < 0 || UNPERM > 100000) {

@@ -287,7 +287,10 @@ int perform_scan(int *geno, chromosome *chrstat, ped *dat, map *genmap, int nid,
     int *bj = (int *)malloc(sizeof(int) * (size_t)(chrint > 0 ? chrint : 1));
     int nb = 0;
     for (int i = s1; i < nchr; i++) {
-        for (int j = (i == s1 ? s2 : 0); j <= i; j++) {
+        /* the reference restarts every later chromosome at column s2 as well
+         * (src/EpiOpenCL.c:1540), skipping blocks (i > s1, j < s2); -R 1 keeps that for
+         * comparisons with its output, the default rescans them */
+        for (int j = (i == s1 || UREFRESUME) ? s2 : 0; j <= i; j++) {
             blocks[nb].start1 = chrstat[i].chrstart;
             blocks[nb].size1 = chrstat[i].chrsize;
             blocks[nb].start2 = chrstat[j].chrstart;

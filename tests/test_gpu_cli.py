@@ -99,6 +99,29 @@ def test_resume_after_interruption(tmp_path):
     assert "Scan already completed" in r.stdout
 
 
+def test_resume_reference_rule(tmp_path):
+    """Interrupted after block (2, 0): the default resume scans (2, 1), (2, 2) and every block of
+    chromosome 3; -R 1 restarts chromosome 3 at column 1 as the reference's loop does
+    (src/EpiOpenCL.c:1540) and so leaves out block (3, 0)."""
+    path, d, codes, phen = make_data(tmp_path, sizes=(50, 70, 40, 30))
+    full = tmp_path / "full.txt"
+    args = ["-t", "f", "-F", "3"]
+    r = subprocess.run([str(CLI), "-A", str(path), str(full), *args], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout
+    header, blocks = parse_results(full)
+    assert [(b[0], b[1]) for b in blocks][3] == (2, 0)
+    keep = 8 + sum(1 + len(b[2]) for b in blocks[:4])
+    text = full.read_text().splitlines(keepends=True)
+    for flag, want in (("0", blocks), ("1", [b for b in blocks if (b[0], b[1]) != (3, 0)])):
+        part = tmp_path / ("part%s.txt" % flag)
+        part.write_text("".join(text[:keep]))
+        r = subprocess.run([str(CLI), "-A", str(path), str(part), *args, "-R", flag], capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stdout
+        _, got = parse_results(part)
+        assert got == want, "-R %s" % flag
+
+
 
 def test_plink_fileset_to_scan(tmp_path):
     """PLINK text in, results out: epiGPU -Dr turns a .ped/.map fileset into a .epigpu file
