@@ -151,26 +151,27 @@ __device__ __forceinline__ double div_fast(double num, double den)
 // the exact integer cell counts n and digit sums si (S = si * sc), and Q = sum of y^2 over
 // the pair's valid individuals. Same quantities as pair_stat, arranged to avoid division
 // chains: reciprocals by rcp_d.
-__device__ __forceinline__ PairStat pair_stat_exact(const int n[9], const long long si[9], double sc, double Q,
+__device__ __forceinline__ PairStat pair_stat_exact(const int n[9], const double si[9], double sc, double Q,
                                                     bool want_int)
 {
+    // si are integers below 2^53 in magnitude (digit sums), so every sum of them is exact
     PairStat r;
     int N = 0, nfac = 0;
-    long long St_i = 0;
+    double St_i = 0.0;
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
         N += n[c];
         St_i += si[c];
         nfac += n[c] > 0;
     }
-    const double St = (double)St_i * sc;
+    const double St = St_i * sc;
     const double m = St * rcp_d((double)N);
     double mc[9], SSB = 0.0;
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
         mc[c] = 0.0;
         if (n[c] > 0) {
-            mc[c] = (double)si[c] * sc * rcp_d((double)n[c]);
+            mc[c] = si[c] * sc * rcp_d((double)n[c]);
             const double d = mc[c] - m;
             SSB = fma((double)n[c] * d, d, SSB);
         }
@@ -185,12 +186,12 @@ __device__ __forceinline__ PairStat pair_stat_exact(const int n[9], const long l
         double row[3], col[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            const long long rs = si[3 * i] + si[3 * i + 1] + si[3 * i + 2];
-            const long long cs = si[i] + si[i + 3] + si[i + 6];
+            const double rs = si[3 * i] + si[3 * i + 1] + si[3 * i + 2];
+            const double cs = si[i] + si[i + 3] + si[i + 6];
             const int rn = n[3 * i] + n[3 * i + 1] + n[3 * i + 2];
             const int cn = n[i] + n[i + 3] + n[i + 6];
-            row[i] = rn > 0 ? (double)rs * sc * rcp_d((double)rn) : 0.0;
-            col[i] = cn > 0 ? (double)cs * sc * rcp_d((double)cn) : 0.0;
+            row[i] = rn > 0 ? rs * sc * rcp_d((double)rn) : 0.0;
+            col[i] = cn > 0 ? cs * sc * rcp_d((double)cn) : 0.0;
         }
         double SSI = 0.0;
 #pragma unroll
@@ -204,6 +205,56 @@ __device__ __forceinline__ PairStat pair_stat_exact(const int n[9], const long l
     }
     return r;
 }
+
+// The same statistics in FP32, as a screen: relative error ~1e-6 for the centred trait and
+// the exact integer cells this gets (no cancellation beyond SSW = Q - ... at large N).
+// A pair whose screened F and F2 are clearly below every threshold and below the running
+// maxima cannot be a hit or a new maximum, and keeps these values; every other pair is
+// recomputed by pair_stat_exact.
+__device__ __forceinline__ void pair_stat_f32(const int n[9], const double si[9], float sc, float Q, bool want_int,
+                                              float &F, float &F2)
+{
+    float N = 0.0f, St = 0.0f, nfac = 0.0f, sf[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        sf[c] = (float)si[c] * sc;
+        N += (float)n[c];
+        St += sf[c];
+        nfac += n[c] > 0 ? 1.0f : 0.0f;
+    }
+    const float m = St * __frcp_rn(N);
+    float mc[9], SSB = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        mc[c] = n[c] > 0 ? sf[c] * __frcp_rn((float)n[c]) : 0.0f;
+        const float d = mc[c] - m;
+        SSB = fmaf((float)n[c] * d, d, SSB);
+    }
+    const float SSW = (Q - St * m) - SSB;
+    const float d1 = nfac - 1.0f, d2 = N - nfac;
+    F = (SSB * d2) / (SSW * d1);
+    F2 = 0.0f;
+    if (want_int) {
+        float row[3], col[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float rn = (float)(n[3 * i] + n[3 * i + 1] + n[3 * i + 2]);
+            const float cn = (float)(n[i] + n[i + 3] + n[i + 6]);
+            row[i] = rn > 0.0f ? (sf[3 * i] + sf[3 * i + 1] + sf[3 * i + 2]) * __frcp_rn(rn) : 0.0f;
+            col[i] = cn > 0.0f ? (sf[i] + sf[i + 3] + sf[i + 6]) * __frcp_rn(cn) : 0.0f;
+        }
+        float SSI = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            const float t = mc[c] - row[c / 3] - col[c % 3] + m;
+            SSI = n[c] > 0 ? fmaf((float)n[c] * t, t, SSI) : SSI;
+        }
+        F2 = (SSI * d2) / (4.0f * SSW);
+    }
+}
+
+// x lowered by the screen's margin (relative 1e-3); -inf and NaN stay as they are
+__device__ __forceinline__ float screen_lo(float x) { return x - 1e-3f * fabsf(x); }
 
 template <int RING>
 __device__ __forceinline__ void advance(uint32_t &slot, uint32_t &phase)
@@ -344,7 +395,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             tc::tc_fence_after();
             const uint32_t acc = tl + acc_col(buf);
             const bool report = a.report_trait < 0 || a.report_trait == t;
+            const bool dumping = t == a.report_trait && (a.dump_counts || a.dump_F);
+            const float t1c = screen_lo(a.t1), t2c = screen_lo(a.t2), scf = (float)sc;
             unsigned int fmx = 0u, f2mx = 0u;  // this thread's largest F, F2 of the tile (encoded)
+            // screen against the CTA's maxima so far (exact values, a lower bound of the final
+            // maxima): a pair that can raise a maximum always takes the exact path
+            const unsigned int m1 = reinterpret_cast<volatile unsigned int *>(smax)[t];
+            const unsigned int m2 = reinterpret_cast<volatile unsigned int *>(smax)[a.ntraits + t];
+            float fmx_f = m1 ? ord2f(m1) : -INFINITY, f2mx_f = m2 ? ord2f(m2) : -INFINITY;
 #pragma unroll 1
             for (int rho = rho0; rho < rho0 + ROUNDS / 2; ++rho) {
                 const int jb = 3 * rho;
@@ -371,7 +429,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 if (valid) {
                     // cells in row-major order, row a' = ga (own), ga+1 (r1), ga+2 (r2) mod 3
                     int n[9];
-                    long long si[9];
+                    double si[9];  // digit sums as exact integers
 #pragma unroll
                     for (int b = 0; b < 3; ++b) {
                         const uint32_t w0[3] = {sel3(v[4 * b], ga), r1[4 * b], r2[4 * b]};
@@ -387,8 +445,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                             const uint32_t c2 = src == 0 ? w2[0] : (src == 1 ? w2[1] : w2[2]);
                             const uint32_t c3 = src == 0 ? w3[0] : (src == 1 ? w3[1] : w3[2]);
                             n[3 * ar + b] = (int)c0;
-                            si[3 * ar + b] = (long long)(int)c1 + 256LL * (long long)(int)c2 +
-                                             65536LL * (long long)(int)c3;
+                            si[3 * ar + b] = fma(65536.0, (double)(int)c3, fma(256.0, (double)(int)c2, (double)(int)c1));
                         }
                     }
                     int npair = 0;
@@ -403,8 +460,24 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                         em += sd * (1LL << (8 * d));
                     }
                     const double Q = fma(qcen, (double)npair, pki) - fma(qstep, (double)em, rmj);
-                    s = pair_stat_exact(n, si, sc, Q, a.test_int != 0);
-                    if (t == a.report_trait && (a.dump_counts || a.dump_F)) {
+                    float Ff, F2f;
+                    pair_stat_f32(n, si, scf, (float)Q, a.test_int != 0, Ff, F2f);
+                    const bool exact = dumping || npair < 256 || !(Ff <= t1c) || !(Ff <= screen_lo(fmx_f)) ||
+                                       (a.test_int && (!(F2f <= t2c) || !(F2f <= screen_lo(f2mx_f))));
+                    if (exact) {
+                        s = pair_stat_exact(n, si, sc, Q, a.test_int != 0);
+                    } else {
+                        // below every threshold and both running maxima by more than the margin
+                        int nfac = 0;
+#pragma unroll
+                        for (int c = 0; c < 9; ++c) nfac += n[c] > 0;
+                        s.nfac = nfac;
+                        s.d1 = nfac - 1;
+                        s.d2 = npair - nfac;
+                        s.F = Ff;
+                        s.F2 = F2f;
+                    }
+                    if (dumping) {
                         const size_t o = (size_t)di * un.bd.size2 + dj;
                         if (a.dump_counts)
 #pragma unroll
@@ -417,8 +490,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 }
                 const bool hit = valid && report && is_hit(a, s);
                 emit_hit(a, hit, un.bd.start1 + di, un.bd.start2 + dj, s, t, un.block);
-                if (valid && s.F == s.F) fmx = max(fmx, f2ord((float)s.F));
-                if (valid && s.F2 == s.F2) f2mx = max(f2mx, f2ord((float)s.F2));
+                if (valid && s.F == s.F) {
+                    fmx = max(fmx, f2ord((float)s.F));
+                    fmx_f = fmaxf(fmx_f, (float)s.F);
+                }
+                if (valid && s.F2 == s.F2) {
+                    f2mx = max(f2mx, f2ord((float)s.F2));
+                    f2mx_f = fmaxf(f2mx_f, (float)s.F2);
+                }
             }
             fold_max_enc(&smax[t], fmx);
             if (a.test_int) fold_max_enc(&smax[a.ntraits + t], f2mx);
