@@ -427,25 +427,23 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 s.nfac = s.d1 = s.d2 = 0;
                 s.F = s.F2 = 0.0;
                 if (valid) {
-                    // cells in row-major order, row a' = ga (own), ga+1 (r1), ga+2 (r2) mod 3
+                    // cells row-major with the genotype rows of SNP i in the order the shuffles
+                    // deliver them: relative row 0 = own (a = ga), 1 = r1 (a = ga+1), 2 = r2
+                    // (a = ga+2, mod 3). F and F2 do not depend on the order of the rows; only
+                    // the count dump below maps them back to a.
                     int n[9];
                     double si[9];  // digit sums as exact integers
 #pragma unroll
                     for (int b = 0; b < 3; ++b) {
-                        const uint32_t w0[3] = {sel3(v[4 * b], ga), r1[4 * b], r2[4 * b]};
-                        const uint32_t w1[3] = {sel3(v[4 * b + 1], ga), r1[4 * b + 1], r2[4 * b + 1]};
-                        const uint32_t w2[3] = {sel3(v[4 * b + 2], ga), r1[4 * b + 2], r2[4 * b + 2]};
-                        const uint32_t w3[3] = {sel3(v[4 * b + 3], ga), r1[4 * b + 3], r2[4 * b + 3]};
+                        const uint32_t c0[3] = {sel3(v[4 * b], ga), r1[4 * b], r2[4 * b]};
+                        const uint32_t c1[3] = {sel3(v[4 * b + 1], ga), r1[4 * b + 1], r2[4 * b + 1]};
+                        const uint32_t c2[3] = {sel3(v[4 * b + 2], ga), r1[4 * b + 2], r2[4 * b + 2]};
+                        const uint32_t c3[3] = {sel3(v[4 * b + 3], ga), r1[4 * b + 3], r2[4 * b + 3]};
 #pragma unroll
-                        for (int ar = 0; ar < 3; ++ar) {
-                            // the source (0 own, 1 r1, 2 r2) holding genotype row ar
-                            const int src = (ar - ga + 3) % 3;
-                            const uint32_t c0 = src == 0 ? w0[0] : (src == 1 ? w0[1] : w0[2]);
-                            const uint32_t c1 = src == 0 ? w1[0] : (src == 1 ? w1[1] : w1[2]);
-                            const uint32_t c2 = src == 0 ? w2[0] : (src == 1 ? w2[1] : w2[2]);
-                            const uint32_t c3 = src == 0 ? w3[0] : (src == 1 ? w3[1] : w3[2]);
-                            n[3 * ar + b] = (int)c0;
-                            si[3 * ar + b] = fma(65536.0, (double)(int)c3, fma(256.0, (double)(int)c2, (double)(int)c1));
+                        for (int r = 0; r < 3; ++r) {
+                            n[3 * r + b] = (int)c0[r];
+                            si[3 * r + b] =
+                                fma(65536.0, (double)(int)c3[r], fma(256.0, (double)(int)c2[r], (double)(int)c1[r]));
                         }
                     }
                     int npair = 0;
@@ -481,7 +479,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                         const size_t o = (size_t)di * un.bd.size2 + dj;
                         if (a.dump_counts)
 #pragma unroll
-                            for (int c = 0; c < 9; ++c) a.dump_counts[9 * o + c] = n[c];
+                            for (int c = 0; c < 9; ++c)  // relative row c/3 is genotype (ga + c/3) mod 3
+                                a.dump_counts[9 * o + 3 * ((ga + c / 3) % 3) + c % 3] = n[c];
                         if (a.dump_F) a.dump_F[o] = (float)s.F;
                         if (a.dump_F2) a.dump_F2[o] = (float)s.F2;
                         if (a.dump_df1) a.dump_df1[o] = s.d1;
