@@ -24,26 +24,29 @@
 // in RM_j, an error of at most qstep / 2 per such individual (qstep = max(ytilde^2) / 2^24).
 // The epilogue forms SSB / SSI / F / F2 in FP64.
 //
-// A comes straight from HBM: the genotype-indicator rows h3 (row 3s + a = [g_s == a] bytes)
-// are TMA-loaded into a 128-byte-swizzled shared-memory stage and read by the MMA from there
-// (no register pass). B is expanded from the j-tile's one-hot genotype bytes and the trait's
-// digit rows by producer warps.
+// The GEMM runs on a CTA pair (a cluster of two CTAs on two SMs, tcgen05 cta_group::2): one
+// MMA of M = 256 rows (each CTA's 40 i-SNPs, 3 genotype rows each, in its own shared memory)
+// by N = 256 columns (the 240 columns of 16 j-SNPs plus 16 zero columns; each CTA holds and
+// builds half of them), so each SM expands half of B per stage. Each CTA's TMEM receives the
+// accumulator rows of its own i-SNPs, which its epilogue reads.
 //
-// Persistent kernel, one CTA per SM, warp-specialised, 14 warps:
-//   warp 13       TMA loader (one thread): per 128-individual stage, the A stage (four 2-D
-//                 tiled loads of 30 h3 rows, into rows 32w..32w+29) and the raw stage (the
-//                 j-tile's 16 one-hot rows and the trait's 7 digit rows); no multicast;
-//                 completion by mbarrier transaction bytes
-//   warps 4-7     B producers: raw j rows x digits -> the stage's B tile (K-major, 128-byte
-//                 swizzle) in smem
-//   warp 12       TMEM allocator and MMA issuer (one thread): 4 x tcgen05.mma (A and B from
-//                 shared memory, N = 240) per stage
-//   warps 0-3, 8-11  epilogue, two warps per TMEM lane quarter, each taking three of the six
-//                 j rounds: tcgen05.ld of the accumulator, lane-triplet shuffles, FP64
-//                 statistics, warp-aggregated hit append, per-trait max F
-// TMEM (512 columns): accumulators at [0, 240) and [240, 480), so the epilogue of one tile
-// overlaps the MMAs of the next. All waits are bounded (tc_ptx.cuh); a timeout sets
-// counters[2] and every role leaves its loop.
+// A comes straight from HBM: the genotype-indicator rows h3 (row 3s + a = [g_s == a] bytes)
+// are TMA-loaded into a 128-byte-swizzled shared-memory stage and read by the MMA from there.
+//
+// Per CTA, 14 warps:
+//   warp 13       TMA loader (one thread): per 128-individual stage, the CTA's A stage (four
+//                 2-D tiled loads of 30 h3 rows into rows 32w..32w+29) and the raw stage (the
+//                 j-tile's 16 one-hot rows and the trait's 7 digit rows); no multicast
+//   warps 4-7     B producers: raw rows -> this CTA's half of the B stage (K-major, 128-byte
+//                 swizzle): CTA 0 column types 0-7, CTA 1 types 8-14
+//   warp 12       CTA 0: MMA issuer (one thread): 4 pair MMAs per stage; CTA 1: forwards the
+//                 completion of its own A stages to CTA 0. Both: TMEM allocation (pair form)
+//   warps 0-3, 8-11  epilogue, two warps per TMEM lane quarter, three j rounds each
+// Handshakes: CTA 0's full / afull / acc_empty barriers also count arrivals from CTA 1; the
+// MMA's commits arrive on both CTAs' empty and acc_full barriers (multicast). TMEM (512
+// columns per CTA): accumulators at [0, 256) and [256, 512). All waits are bounded
+// (tc_ptx.cuh); a timeout sets counters[2] and every role leaves its loop; the CTAs meet in
+// a cluster barrier before the TMEM is released.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -53,25 +56,27 @@
 namespace epi {
 namespace mma {
 
-constexpr int TI = 40;         // i-SNPs per tile (4 lane quarters x 10 triplets)
+constexpr int TI = 40;         // i-SNPs per CTA (4 lane quarters x 10 triplets)
+constexpr int TIP = 2 * TI;    // i-SNPs per pair tile
 constexpr int TJ = 16;         // j-SNPs per tile
 constexpr int NTY = 12;        // B column types per j-SNP: b (3) x {w, d0, d1, d2} ...
 constexpr int NTYPE = 15;      // ... and missing x {e0, e1, e2}
-constexpr int N = TJ * NTYPE;  // 240
-constexpr int M = 128;
+constexpr int NCOL = TJ * NTYPE;  // 240 columns in use
+constexpr int N = 256;         // MMA width (pair MMAs take multiples of 32); columns 240-255 zero
+constexpr int NH = N / 2;      // B columns held by each CTA
+constexpr int M = 256;         // MMA height over the pair
 constexpr int KS = 128;        // individuals per pipeline stage
-constexpr int STAGES = 4;      // B ring (smem)
-constexpr int ASTAGES = 4;     // A ring (smem, TMA)
+constexpr int STAGES = 5;      // operand ring (A and B of a stage share the slot index)
 constexpr int RSTAGES = 6;     // raw ring (smem, TMA)
 constexpr int ND = 7;          // digit rows per trait: w, Y digits (3), E digits (3)
 constexpr int ROUNDS = (TJ + 2) / 3;  // j rounds of the epilogue (3 j-SNPs per round)
 constexpr uint32_t ACC_COL1 = N;
 __host__ __device__ constexpr uint32_t acc_col(uint32_t buf) { return buf ? ACC_COL1 : 0u; }
 constexpr uint32_t TMEM_COLS = 512;
-constexpr int A_STAGE = M * KS;  // 16 KB
-constexpr int B_STAGE = N * KS;  // 30 KB
-constexpr int A_BOX = 30;        // h3 rows per TMA box (10 i-SNPs x 3 genotypes)
-constexpr uint32_t A_BYTES = 4 * A_BOX * KS;  // transaction bytes per A stage
+constexpr int A_STAGE = (M / 2) * KS;  // 16 KB
+constexpr int B_STAGE = NH * KS;       // 16 KB
+constexpr int A_BOX = 30;              // h3 rows per TMA box (10 i-SNPs x 3 genotypes)
+constexpr uint32_t A_BYTES = 4 * A_BOX * KS;  // transaction bytes per A stage (one CTA)
 // raw stage: the j-tile's one-hot rows and the trait's digit rows, 1024-aligned sections
 constexpr int RAW_J = 0, RAW_D = TJ * KS;
 constexpr int RAW_STAGE = 4 * 1024;
@@ -80,14 +85,17 @@ constexpr int NWARPS = 14;
 constexpr int NTHREADS = NWARPS * 32;
 constexpr uint32_t IDESC = tc::idesc_i8(M, N);
 static_assert(RAW_D % 1024 == 0 && RAW_D + ND * KS <= RAW_STAGE, "raw layout");
-static_assert(B_STAGE % 1024 == 0 && A_STAGE % 1024 == 0 && N % 16 == 0 && N <= 256, "operand tiles");
+static_assert(B_STAGE % 1024 == 0 && A_STAGE % 1024 == 0 && N % 32 == 0 && N <= 256 && NCOL <= N, "operand tiles");
+static_assert(NCOL - NH == 7 * TJ && NH == 8 * TJ, "B split: CTA 0 types 0-7, CTA 1 types 8-14 + padding");
 static_assert(2 * N <= (int)TMEM_COLS && ROUNDS % 2 == 0, "TMEM layout / epilogue split");
 
 struct Smem {
-    uint8_t a[ASTAGES][A_STAGE];
+    uint8_t a[STAGES][A_STAGE];
     uint8_t b[STAGES][B_STAGE];
     uint8_t raw[RSTAGES][RAW_STAGE];
-    uint64_t full[STAGES], empty[STAGES], afull[ASTAGES], aempty[ASTAGES], raw_full[RSTAGES], raw_empty[RSTAGES],
+    // full: B halves built (CTA 0: 4 local + 4 remote producer warps); afull: A stages landed
+    // (CTA 0: own TMA + CTA 1's forward; CTA 1: own TMA); empty: MMAs of the slot done (both)
+    uint64_t full[STAGES], empty[STAGES], afull[STAGES], raw_full[RSTAGES], raw_empty[RSTAGES],
         acc_full[2], acc_empty[2], drain;
     uint32_t tmem_base;
     int abort;
@@ -113,9 +121,9 @@ __device__ __forceinline__ Unit decode(const ScanArgs &a, long long u)
     r.block = find_block(a.blocks, a.nblocks, tile);
     r.bd = a.blocks[r.block];
     const long long lt = tile - r.bd.tile_base;
-    r.i0 = (int)(lt / r.bd.tiles_j) * TI;
+    r.i0 = (int)(lt / r.bd.tiles_j) * TIP;  // the pair tile's first i-SNP
     r.j0 = (int)(lt % r.bd.tiles_j) * TJ;
-    r.skip = r.bd.start1 + min(r.i0 + TI, r.bd.size1) - 1 <= r.bd.start2 + r.j0;
+    r.skip = r.bd.start1 + min(r.i0 + TIP, r.bd.size1) - 1 <= r.bd.start2 + r.j0;
     return r;
 }
 
@@ -268,28 +276,35 @@ __device__ __forceinline__ void advance(uint32_t &slot, uint32_t &phase)
 __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __grid_constant__ MmaMaps maps)
 {
     extern __shared__ uint8_t smem_raw[];
-    // the operand stages need 1024-byte alignment (128-byte swizzle atoms)
+    // the operand stages need 1024-byte alignment (128-byte swizzle atoms); the offset is the
+    // same in both CTAs of the pair, as the pair MMA and the remote arrivals require
     const uint32_t raw_s = tc::smem_u32(smem_raw);
     Smem &sm = *reinterpret_cast<Smem *>(smem_raw + (((raw_s + 1023u) & ~1023u) - raw_s));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = tc::cluster_rank();  // 0: issues the MMAs
+    const long long pair = tc::cluster_id(), npairs = tc::cluster_count();
     const long long units = a.ntiles * (long long)a.ntraits;
     const int nks = a.Np / KS;
 
     if (warp == 12) {
-        tc::tmem_alloc(&sm.tmem_base, TMEM_COLS);
-        tc::tmem_relinquish();
+        tc::tmem_alloc_pair(&sm.tmem_base, TMEM_COLS);
+        tc::tmem_relinquish_pair();
     }
+    // CTA 1 holds B columns 128-255: its rows 112-127 (columns 240-255) stay zero
+    if (rank == 1)
+        for (int w = threadIdx.x; w < STAGES * (NH - (NCOL - NH)) * 8; w += blockDim.x) {
+            const int st = w / ((NH - (NCOL - NH)) * 8), n = (NCOL - NH) + (w / 8) % (NH - (NCOL - NH)), c = w % 8;
+            *reinterpret_cast<uint4 *>(sm.b[st] + (n >> 3) * 1024 + (n & 7) * 128 + c * 16) = make_uint4(0, 0, 0, 0);
+        }
+    tc::fence_proxy_async_smem();
     // per-CTA maxima of F and F2 per trait (flushed to global memory once, at the end)
     unsigned int *smax = reinterpret_cast<unsigned int *>(reinterpret_cast<uint8_t *>(&sm) + sizeof(Smem));
     for (int w = threadIdx.x; w < 2 * a.ntraits; w += blockDim.x) smax[w] = 0u;
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
-            tc::mbar_init(&sm.full[s], 4);
+            tc::mbar_init(&sm.full[s], rank == 0 ? 8 : 1);
             tc::mbar_init(&sm.empty[s], 1);
-        }
-        for (int s = 0; s < ASTAGES; ++s) {
-            tc::mbar_init(&sm.afull[s], 1);
-            tc::mbar_init(&sm.aempty[s], 1);
+            tc::mbar_init(&sm.afull[s], rank == 0 ? 2 : 1);
         }
         for (int r = 0; r < RSTAGES; ++r) {
             tc::mbar_init(&sm.raw_full[r], 1);
@@ -297,7 +312,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         }
         for (int b = 0; b < 2; ++b) {
             tc::mbar_init(&sm.acc_full[b], 1);
-            tc::mbar_init(&sm.acc_empty[b], 8);
+            tc::mbar_init(&sm.acc_empty[b], 16);
         }
         tc::mbar_init(&sm.drain, 1);
         sm.abort = 0;
@@ -305,6 +320,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
     }
     tc::tc_fence_before();
     __syncthreads();
+    tc::cluster_sync();  // both CTAs' barriers exist before any remote arrival
     tc::tc_fence_after();
     const uint32_t tmem = sm.tmem_base;
     volatile int *abort = &sm.abort;
@@ -314,7 +330,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         const int t = threadIdx.x - 128, jj = t >> 3, c = t & 7;
         uint32_t stage = 0, phase = 0, rs = 0, rph = 0;
         bool ok = true;
-        for (long long u = blockIdx.x; u < units && ok; u += gridDim.x) {
+        for (long long u = pair; u < units && ok; u += npairs) {
             const Unit un = decode(a, u);
             if (un.skip) continue;
             for (int ks = 0; ks < nks; ++ks) {
@@ -325,12 +341,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 }
                 const uint8_t *raw = sm.raw[rs];
                 const uint4 h = ld_sw128(raw + RAW_J, jj, c);
-                uint4 d[ND];
-#pragma unroll
-                for (int s2 = 0; s2 < ND; ++s2) d[s2] = ld_sw128(raw + RAW_D, s2, c);
                 uint8_t *base = sm.b[stage];
+                // column type ty of this CTA's half at local row (ty - 8 rank) * 16 + jj
                 auto put = [&](int ty, const uint4 &m, const uint4 &dv) {
-                    const int n = ty * TJ + jj;
+                    const int n = (ty - 8 * (int)rank) * TJ + jj;
                     uint4 o;
                     o.x = m.x & dv.x;
                     o.y = m.y & dv.y;
@@ -338,33 +352,52 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     o.w = m.w & dv.w;
                     *reinterpret_cast<uint4 *>(base + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4)) = o;
                 };
+                if (rank == 0) {
+                    // types 0-7: genotypes 0 and 1 x {w, d0, d1, d2}
+                    uint4 d[4];
 #pragma unroll
-                for (int b = 0; b < 3; ++b) {
+                    for (int s2 = 0; s2 < 4; ++s2) d[s2] = ld_sw128(raw + RAW_D, s2, c);
+#pragma unroll
+                    for (int b = 0; b < 2; ++b) {
+                        uint4 m;
+                        m.x = ((h.x >> b) & 0x01010101u) * 0xFFu;
+                        m.y = ((h.y >> b) & 0x01010101u) * 0xFFu;
+                        m.z = ((h.z >> b) & 0x01010101u) * 0xFFu;
+                        m.w = ((h.w >> b) & 0x01010101u) * 0xFFu;
+#pragma unroll
+                        for (int s2 = 0; s2 < 4; ++s2) put(4 * b + s2, m, d[s2]);
+                    }
+                } else {
+                    // types 8-11: genotype 2 x {w, d0, d1, d2}; 12-14: missing x {e0, e1, e2}
+                    uint4 d[ND];
+#pragma unroll
+                    for (int s2 = 0; s2 < ND; ++s2) d[s2] = ld_sw128(raw + RAW_D, s2, c);
                     uint4 m;
-                    m.x = ((h.x >> b) & 0x01010101u) * 0xFFu;
-                    m.y = ((h.y >> b) & 0x01010101u) * 0xFFu;
-                    m.z = ((h.z >> b) & 0x01010101u) * 0xFFu;
-                    m.w = ((h.w >> b) & 0x01010101u) * 0xFFu;
+                    m.x = ((h.x >> 2) & 0x01010101u) * 0xFFu;
+                    m.y = ((h.y >> 2) & 0x01010101u) * 0xFFu;
+                    m.z = ((h.z >> 2) & 0x01010101u) * 0xFFu;
+                    m.w = ((h.w >> 2) & 0x01010101u) * 0xFFu;
 #pragma unroll
-                    for (int s2 = 0; s2 < 4; ++s2) put(4 * b + s2, m, d[s2]);
+                    for (int s2 = 0; s2 < 4; ++s2) put(8 + s2, m, d[s2]);
+                    // missing genotype: one-hot byte 0 (bits 0-2 clear); the shifts only move
+                    // bits of the next byte into bits 6-7 of this one, which the mask drops
+                    uint4 mm;
+                    mm.x = (((h.x | (h.x >> 1) | (h.x >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
+                    mm.y = (((h.y | (h.y >> 1) | (h.y >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
+                    mm.z = (((h.z | (h.z >> 1) | (h.z >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
+                    mm.w = (((h.w | (h.w >> 1) | (h.w >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
+                    put(12, mm, d[4]);
+                    put(13, mm, d[5]);
+                    put(14, mm, d[6]);
                 }
-                // missing genotype: one-hot byte 0 (bits 0-2 clear); the shifts only move
-                // bits of the next byte into bits 6-7 of this one, which the mask drops
-                uint4 mm;
-                mm.x = (((h.x | (h.x >> 1) | (h.x >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
-                mm.y = (((h.y | (h.y >> 1) | (h.y >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
-                mm.z = (((h.z | (h.z >> 1) | (h.z >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
-                mm.w = (((h.w | (h.w >> 1) | (h.w >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
-                put(12, mm, d[4]);
-                put(13, mm, d[5]);
-                put(14, mm, d[6]);
                 // the raw slot is released only after the stores above, which consume every
                 // value loaded from it (an arrive right after the loads can overtake them)
                 tc::fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) {
                     tc::mbar_arrive(&sm.raw_empty[rs]);
-                    tc::mbar_arrive(&sm.full[stage]);
+                    if (rank == 0) tc::mbar_arrive(&sm.full[stage]);
+                    else tc::mbar_arrive_remote(&sm.full[stage], 0);
                 }
                 advance<STAGES>(stage, phase);
                 advance<RSTAGES>(rs, rph);
@@ -378,9 +411,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         const uint32_t tl = tmem + ((uint32_t)(32 * e) << 16);
         uint32_t accph[2] = {0u, 0u};
         int buf = 0;
-        for (long long u = blockIdx.x; u < units; u += gridDim.x) {
-            const Unit un = decode(a, u);
+        for (long long u = pair; u < units; u += npairs) {
+            Unit un = decode(a, u);
             if (un.skip) continue;
+            un.i0 += TI * (int)rank;  // this CTA's i-SNPs
             const int t = un.trait;
             const double sc = a.yscale[t], qcen = a.qcen[t], qstep = a.qstep[t];
             const int di = un.i0 + ii;
@@ -502,7 +536,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             if (a.test_int) fold_max_enc(&smax[a.ntraits + t], f2mx);
             tc::tc_fence_before();
             __syncwarp();
-            if (lane == 0) tc::mbar_arrive(&sm.acc_empty[buf]);
+            if (lane == 0) {
+                if (rank == 0) tc::mbar_arrive(&sm.acc_empty[buf]);
+                else tc::mbar_arrive_remote(&sm.acc_empty[buf], 0);
+            }
             accph[buf] ^= 1u;
             buf ^= 1;
         }
@@ -511,12 +548,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         if (lane == 0) {
             uint32_t as = 0, aph = 0, rs = 0, rph = 0, issued_a = 0, issued_r = 0;
             bool ok = true;
-            for (long long u = blockIdx.x; u < units && ok; u += gridDim.x) {
+            for (long long u = pair; u < units && ok; u += npairs) {
                 const Unit un = decode(a, u);
                 if (un.skip) continue;
-                const int arow = 3 * (un.bd.start1 + un.i0);
+                const int arow = 3 * (un.bd.start1 + un.i0 + TI * (int)rank);
                 for (int ks = 0; ks < nks; ++ks) {
-                    if (!tc::mbar_wait(&sm.aempty[as], aph ^ 1u, abort)) {
+                    if (!tc::mbar_wait(&sm.empty[as], aph ^ 1u, abort)) {
                         fail(a, sm, 7);
                         ok = false;
                         break;
@@ -526,7 +563,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     for (int w = 0; w < 4; ++w)
                         tc::tma_load_2d(sm.a[as] + 32 * w * KS, &maps.hi, ks * KS, arow + A_BOX * w, &sm.afull[as]);
                     ++issued_a;
-                    advance<ASTAGES>(as, aph);
+                    advance<STAGES>(as, aph);
                     if (!tc::mbar_wait(&sm.raw_empty[rs], rph ^ 1u, abort)) {
                         fail(a, sm, 7);
                         ok = false;
@@ -541,12 +578,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 }
             }
             // no TMA write may still be landing in shared memory when the CTA exits: wait for
-            // the last load issued into every ring slot (already complete on the normal path).
-            // The load issued `back` loads ago went to slot (next - back) and completes the
-            // parity of the current lap, or of the previous one when it wrapped.
+            // the last loads issued into every ring slot. The raw stages complete on local
+            // barriers; A stages of CTA 1 do too, CTA 0's also need CTA 1's forward, so CTA 0
+            // waits for its own bytes only through the phases it can observe (all its
+            // issued phases complete on the normal path; after an abort the bounded wait ends).
             int no_abort = 0;
-            for (uint32_t back = 1; back <= ASTAGES && back <= issued_a; ++back) {
-                const uint32_t slot = (as + ASTAGES - back) % ASTAGES, par = back > as ? (aph ^ 1u) : aph;
+            for (uint32_t back = 1; back <= STAGES && back <= issued_a; ++back) {
+                const uint32_t slot = (as + STAGES - back) % STAGES, par = back > as ? (aph ^ 1u) : aph;
                 if (!tc::mbar_wait(&sm.afull[slot], par, &no_abort)) fail(a, sm, 8);
             }
             for (uint32_t back = 1; back <= RSTAGES && back <= issued_r; ++back) {
@@ -554,54 +592,73 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 if (!tc::mbar_wait(&sm.raw_full[slot], par, &no_abort)) fail(a, sm, 8);
             }
         }
-    } else if (lane == 0) {
-        // ---------------- MMA issuer (warp 12) ----------------
-        uint32_t stage = 0, phase = 0, as = 0, aph = 0, accph[2] = {0u, 0u};
-        int buf = 0;
+    } else if (lane == 0 && rank == 1) {
+        // ---------------- A forwarder (CTA 1, warp 12) ----------------
+        // each of this CTA's A stages, once landed, counts as one arrival on CTA 0's afull
+        uint32_t as = 0, aph = 0;
         bool ok = true;
-        for (long long u = blockIdx.x; u < units && ok; u += gridDim.x) {
+        for (long long u = pair; u < units && ok; u += npairs) {
             const Unit un = decode(a, u);
             if (un.skip) continue;
-            if (!tc::mbar_wait(&sm.acc_empty[buf], accph[buf] ^ 1u, abort)) {
+            for (int ks = 0; ks < nks; ++ks) {
+                if (!tc::mbar_wait(&sm.afull[as], aph, abort)) {
+                    fail(a, sm, 9);
+                    ok = false;
+                    break;
+                }
+                tc::mbar_arrive_remote(&sm.afull[as], 0);
+                advance<STAGES>(as, aph);
+            }
+        }
+    } else if (lane == 0) {
+        // ---------------- MMA issuer (CTA 0, warp 12) ----------------
+        uint32_t stage = 0, phase = 0, accph[2] = {0u, 0u};
+        int buf = 0;
+        bool ok = true;
+        for (long long u = pair; u < units && ok; u += npairs) {
+            const Unit un = decode(a, u);
+            if (un.skip) continue;
+            if (!tc::mbar_wait_cluster(&sm.acc_empty[buf], accph[buf] ^ 1u, abort)) {
                 fail(a, sm, 4);
                 break;
             }
             tc::tc_fence_after();
             const uint32_t d = tmem + acc_col(buf);
             for (int ks = 0; ks < nks; ++ks) {
-                if (!tc::mbar_wait(&sm.full[stage], phase, abort) || !tc::mbar_wait(&sm.afull[as], aph, abort)) {
+                if (!tc::mbar_wait_cluster(&sm.full[stage], phase, abort) ||
+                    !tc::mbar_wait_cluster(&sm.afull[stage], phase, abort)) {
                     fail(a, sm, 5);
                     ok = false;
                     break;
                 }
                 tc::tc_fence_after();
-                const uint32_t asb = tc::smem_u32(sm.a[as]), bsb = tc::smem_u32(sm.b[stage]);
+                const uint32_t asb = tc::smem_u32(sm.a[stage]), bsb = tc::smem_u32(sm.b[stage]);
 #pragma unroll
                 for (int kk = 0; kk < KS / 32; ++kk)
-                    tc::mma_i8_ss(d, tc::smem_desc_sw128(asb + 32 * kk), tc::smem_desc_sw128(bsb + 32 * kk), IDESC,
-                                  (ks | kk) != 0);
-                tc::mma_commit(&sm.empty[stage]);
-                tc::mma_commit(&sm.aempty[as]);
+                    tc::mma_i8_pair(d, tc::smem_desc_sw128(asb + 32 * kk), tc::smem_desc_sw128(bsb + 32 * kk), IDESC,
+                                    (ks | kk) != 0);
+                tc::mma_commit_pair_mc(&sm.empty[stage], 0x3);
                 advance<STAGES>(stage, phase);
-                advance<ASTAGES>(as, aph);
             }
             if (!ok) break;
-            tc::mma_commit(&sm.acc_full[buf]);
+            tc::mma_commit_pair_mc(&sm.acc_full[buf], 0x3);
             accph[buf] ^= 1u;
             buf ^= 1;
         }
         // every MMA issued above has completed once `drain` flips (waited for even after an
-        // abort: the accumulators must be idle before the TMEM is released)
-        tc::mma_commit(&sm.drain);
+        // abort: the accumulators and both CTAs' operands must be idle before the TMEM and
+        // shared memory are released)
+        tc::mma_commit_pair(&sm.drain);
         int no_abort = 0;
         if (!tc::mbar_wait(&sm.drain, 0, &no_abort)) fail(a, sm, 6);
     }
 
     tc::tc_fence_before();
     __syncthreads();
+    tc::cluster_sync();  // CTA 0's MMAs (which read CTA 1's shared memory) have drained
     if (warp == 12) {
         tc::tc_fence_after();
-        tc::tmem_dealloc(tmem, TMEM_COLS);
+        tc::tmem_dealloc_pair(tmem, TMEM_COLS);
     }
     for (int w = threadIdx.x; w < 2 * a.ntraits; w += blockDim.x)
         if (smax[w]) atomicMax(w < a.ntraits ? &a.maxf[w] : &a.maxf2[w - a.ntraits], smax[w]);
@@ -646,7 +703,7 @@ cudaError_t mma_encode_traits(MmaMaps *maps, const int8_t *ydig, int ntraits, in
 }
 
 bool mma_available() { return true; }
-int mma_tile_i() { return mma::TI; }
+int mma_tile_i() { return mma::TIP; }  // the host tiles blocks by CTA-pair tiles
 int mma_tile_j() { return mma::TJ; }
 int mma_min_nid() { return 256; }
 int mma_max_nid() { return 1 << 24; }  // digit sums stay within int32
@@ -654,13 +711,31 @@ int mma_stage_individuals() { return mma::KS; }
 
 cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream)
 {
-    // more than half of the SM's shared memory: one CTA per SM, which owns all 512 TMEM columns;
-    // the tail holds the per-CTA maxima
+    // more than half of the SM's shared memory: one CTA per SM, which owns all 512 TMEM
+    // columns; the tail holds the per-CTA maxima. CTAs run in clusters of two (the pair MMA).
     const size_t smem = sizeof(mma::Smem) + 1024 + 8 * (size_t)a.ntraits;
     static_assert(sizeof(mma::Smem) + 1024 > 116 * 1024, "one CTA per SM");
     cudaError_t e = cudaFuncSetAttribute(mma::k_scan_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    mma::k_scan_mma<<<grid, mma::NTHREADS, smem, stream>>>(a, maps);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)(grid & ~1), 1, 1);
+    cfg.blockDim = dim3(mma::NTHREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    e = cudaOccupancyMaxActiveClusters(&clusters, mma::k_scan_mma, &cfg);
+    if (e != cudaSuccess) return e;
+    if (clusters < 1) return cudaErrorInvalidConfiguration;
+    if (2 * clusters < (int)cfg.gridDim.x) cfg.gridDim.x = 2 * (unsigned)clusters;
+    e = cudaLaunchKernelEx(&cfg, mma::k_scan_mma, a, maps);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
