@@ -143,6 +143,11 @@ class ClockSampler:
             self.t.start()
         except OSError:
             self.proc = None
+        # nvidia-smi's start-up (driver queries) must not overlap a short timed region: wait
+        # for its first sample
+        t0 = time.time()
+        while self.proc and not self.lines and self.proc.poll() is None and time.time() - t0 < 5.0:
+            time.sleep(0.01)
         return self
 
     def _read(self):
@@ -402,15 +407,17 @@ def main():
         if used_form == "tensor":
             int8 = int8_peak_tops()
             # algorithmic int8 ops per pair: 3 genotype rows x 15 column types (3 x {count, 3 y
-            # digits} + 3 y^2 digits) per individual; the 128 x 240 tile carries 48 (padding rows)
+            # digits} + 3 y^2 digits) per individual; the 256 x 256 pair tile carries 51.2
+            # (8 padding rows per CTA, 16 zero columns)
             ops_pair = 2.0 * 45.0 * nid
             achieved = pairs_launch * ops_pair / kern_s / 1e12
             # DRAM bytes per launch: the ncu capture of the same kernel on the cfg3m workload
-            # (N=10,000, M=20,000, operands larger than L2) read 13.178 GB for 199,990,000
-            # pairs over Np = 10,112 padded individuals; the j rows are streamed once per i
-            # tile, so the bytes scale with pairs x Np (profiles/scan_mma_traffic_cfg3m.md)
+            # (N=10,000, M=20,000, operands larger than L2) read and wrote 18.33 GB for
+            # 199,990,000 pairs over Np = 10,112 padded individuals; the j rows are streamed
+            # once per i tile, so the bytes scale with pairs x Np
+            # (profiles/scan_mma_traffic_cfg3m.md)
             np_pad = (nid + 127) // 128 * 128
-            traffic = 13.178e9 / (199990000.0 * 10112.0) * pairs_launch * np_pad
+            traffic = 18.33e9 / (199990000.0 * 10112.0) * pairs_launch * np_pad
             roof = {"bound": "tensor", "achieved": achieved, "peak": int8, "unit": "TOP/s",
                     "frac": achieved / int8, "traffic": traffic, "traffic_unit": "bytes per launch",
                     "traffic_source": "ncu dram__bytes_read+write on cfg3m, scaled by pairs x individuals",
