@@ -62,7 +62,8 @@ struct epi_ctx {
     uint32_t *d_wmask = nullptr;
     double *d_qc = nullptr, *d_yscale = nullptr, *d_qd = nullptr, *d_qtot = nullptr, *d_qm = nullptr;
     int8_t *d_ydig = nullptr;
-    size_t traits_cap = 0, ydig_cap = 0, qd_cap = 0, qm_cap = 0;
+    size_t traits_cap = 0, ydig_cap = 0, qd_cap = 0, qm_cap = 0, wmask_cap = 0, qc_cap = 0, qtot_cap = 0,
+           yscale_cap = 0;
     bool qm_valid = false;
     epi::MmaMaps maps;
     std::vector<double> qc;
@@ -342,26 +343,18 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
     CK(ensure(&ctx->d_y, &cap_y, need));
     CK(ensure(&ctx->d_q, &cap_q, need));
     ctx->traits_cap = std::min(cap_y, cap_q);
-    size_t cw = 0, cq = 0;
-    if (ctx->d_wmask) cudaFree(ctx->d_wmask);
-    if (ctx->d_qc) cudaFree(ctx->d_qc);
-    ctx->d_wmask = nullptr;
-    ctx->d_qc = nullptr;
-    CK(ensure(&ctx->d_wmask, &cw, (size_t)ntraits * Wp * sizeof(uint32_t)));
-    CK(ensure(&ctx->d_qc, &cq, (size_t)ntraits * sizeof(double)));
+    // buffers are kept across calls while they are large enough: a cudaFree would
+    // synchronise the device on every trait upload
+    CK(ensure(&ctx->d_wmask, &ctx->wmask_cap, (size_t)ntraits * Wp * sizeof(uint32_t)));
+    CK(ensure(&ctx->d_qc, &ctx->qc_cap, (size_t)ntraits * sizeof(double)));
     CK(cudaMemcpyAsync(ctx->d_y, hy.data(), need, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->d_q, hq.data(), need, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->d_wmask, hw.data(), hw.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->d_qc, ctx->qc.data(), ntraits * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(ensure(&ctx->d_ydig, &ctx->ydig_cap, hd.size()));
     CK(ensure(&ctx->d_qd, &ctx->qd_cap, hqd.size() * sizeof(double)));
-    if (ctx->d_qtot) cudaFree(ctx->d_qtot);
-    if (ctx->d_yscale) cudaFree(ctx->d_yscale);
-    ctx->d_qtot = nullptr;
-    ctx->d_yscale = nullptr;
-    size_t c1 = 0, c2 = 0;
-    CK(ensure(&ctx->d_qtot, &c1, (size_t)ntraits * sizeof(double)));
-    CK(ensure(&ctx->d_yscale, &c2, hsc.size() * sizeof(double)));
+    CK(ensure(&ctx->d_qtot, &ctx->qtot_cap, (size_t)ntraits * sizeof(double)));
+    CK(ensure(&ctx->d_yscale, &ctx->yscale_cap, hsc.size() * sizeof(double)));
     CK(cudaMemcpyAsync(ctx->d_ydig, hd.data(), hd.size(), cudaMemcpyHostToDevice, ctx->stream));
     CK(epi::mma_encode_traits(&ctx->maps, ctx->d_ydig, ntraits, Np));
     CK(cudaMemcpyAsync(ctx->d_qd, hqd.data(), hqd.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));

@@ -28,6 +28,15 @@
 
 namespace epi {
 
+// The scan kernels keep per-CTA maxima of F and F2 in shared memory (8 bytes per trait,
+// flushed to global memory once per CTA) for up to this many traits; larger trait sets (a
+// permutation run of thousands of phenotypes) fold straight into the global maxima.
+constexpr int SMAX_TRAITS = 512;
+__host__ __device__ constexpr size_t smax_bytes(int ntraits)
+{
+    return ntraits <= SMAX_TRAITS ? 8 * (size_t)ntraits : 0;
+}
+
 // One hit as written by a kernel; sorted into the reference's output order on the host.
 struct DevHit {
     int32_t snp1, snp2, df1, df2;

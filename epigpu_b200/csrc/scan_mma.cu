@@ -33,10 +33,11 @@
 // A comes straight from HBM: the genotype-indicator rows h3 (row 3s + a = [g_s == a] bytes)
 // are TMA-loaded into a 128-byte-swizzled shared-memory stage and read by the MMA from there.
 //
-// Per CTA, 14 warps:
-//   warp 13       TMA loader (one thread): per 128-individual stage, the CTA's A stage (four
-//                 2-D tiled loads of 30 h3 rows into rows 32w..32w+29) and the raw stage (the
-//                 j-tile's 16 one-hot rows and the trait's 7 digit rows); no multicast
+// Per CTA, 15 warps:
+//   warp 13       A loader (one thread): per 128-individual stage, the CTA's A stage (four
+//                 2-D tiled loads of 30 h3 rows into rows 32w..32w+29); no multicast
+//   warp 14       raw loader (one thread): per stage, the j-tile's 16 one-hot rows and the
+//                 trait's 7 digit rows, up to RSTAGES stages ahead of the B producers
 //   warps 4-7     B producers: raw rows -> this CTA's half of the B stage (K-major, 128-byte
 //                 swizzle): CTA 0 column types 0-7, CTA 1 types 8-14
 //   warp 12       CTA 0: MMA issuer (one thread): 4 pair MMAs per stage; CTA 1: forwards the
@@ -67,7 +68,7 @@ constexpr int NH = N / 2;      // B columns held by each CTA
 constexpr int M = 256;         // MMA height over the pair
 constexpr int KS = 128;        // individuals per pipeline stage
 constexpr int STAGES = 5;      // operand ring (A and B of a stage share the slot index)
-constexpr int RSTAGES = 6;     // raw ring (smem, TMA)
+constexpr int RSTAGES = 10;    // raw ring (smem, TMA)
 constexpr int ND = 7;          // digit rows per trait: w, Y digits (3), E digits (3)
 constexpr int ROUNDS = (TJ + 2) / 3;  // j rounds of the epilogue (3 j-SNPs per round)
 constexpr uint32_t ACC_COL1 = N;
@@ -81,7 +82,7 @@ constexpr uint32_t A_BYTES = 4 * A_BOX * KS;  // transaction bytes per A stage (
 constexpr int RAW_J = 0, RAW_D = TJ * KS;
 constexpr int RAW_STAGE = 4 * 1024;
 constexpr uint32_t RAW_BYTES = (TJ + ND) * KS;
-constexpr int NWARPS = 14;
+constexpr int NWARPS = 15;
 constexpr int NTHREADS = NWARPS * 32;
 constexpr uint32_t IDESC = tc::idesc_i8(M, N);
 static_assert(RAW_D % 1024 == 0 && RAW_D + ND * KS <= RAW_STAGE, "raw layout");
@@ -297,9 +298,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             *reinterpret_cast<uint4 *>(sm.b[st] + (n >> 3) * 1024 + (n & 7) * 128 + c * 16) = make_uint4(0, 0, 0, 0);
         }
     tc::fence_proxy_async_smem();
-    // per-CTA maxima of F and F2 per trait (flushed to global memory once, at the end)
+    // maxima of F and F2 per trait: per CTA in shared memory (flushed to global memory once,
+    // at the end) up to SMAX_TRAITS traits, else the global maxima directly
+    const bool smax_local = a.ntraits <= SMAX_TRAITS;
     unsigned int *smax = reinterpret_cast<unsigned int *>(reinterpret_cast<uint8_t *>(&sm) + sizeof(Smem));
-    for (int w = threadIdx.x; w < 2 * a.ntraits; w += blockDim.x) smax[w] = 0u;
+    if (smax_local)
+        for (int w = threadIdx.x; w < 2 * a.ntraits; w += blockDim.x) smax[w] = 0u;
+    unsigned int *const mxf = smax_local ? smax : a.maxf;
+    unsigned int *const mxf2 = smax_local ? smax + a.ntraits : a.maxf2;
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
             tc::mbar_init(&sm.full[s], rank == 0 ? 8 : 1);
@@ -434,8 +440,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             unsigned int fmx = 0u, f2mx = 0u;  // this thread's largest F, F2 of the tile (encoded)
             // screen against the CTA's maxima so far (exact values, a lower bound of the final
             // maxima): a pair that can raise a maximum always takes the exact path
-            const unsigned int m1 = reinterpret_cast<volatile unsigned int *>(smax)[t];
-            const unsigned int m2 = reinterpret_cast<volatile unsigned int *>(smax)[a.ntraits + t];
+            const unsigned int m1 = reinterpret_cast<volatile unsigned int *>(mxf)[t];
+            const unsigned int m2 = reinterpret_cast<volatile unsigned int *>(mxf2)[t];
             float fmx_f = m1 ? ord2f(m1) : -INFINITY, f2mx_f = m2 ? ord2f(m2) : -INFINITY;
 #pragma unroll 1
             for (int rho = rho0; rho < rho0 + ROUNDS / 2; ++rho) {
@@ -532,8 +538,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     f2mx_f = fmaxf(f2mx_f, (float)s.F2);
                 }
             }
-            fold_max_enc(&smax[t], fmx);
-            if (a.test_int) fold_max_enc(&smax[a.ntraits + t], f2mx);
+            fold_max_enc(&mxf[t], fmx);
+            if (a.test_int) fold_max_enc(&mxf2[t], f2mx);
             tc::tc_fence_before();
             __syncwarp();
             if (lane == 0) {
@@ -544,9 +550,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             buf ^= 1;
         }
     } else if (warp == 13) {
-        // ---------------- TMA loader ----------------
+        // ---------------- A loader: this CTA's indicator rows, one slot per operand stage ----
         if (lane == 0) {
-            uint32_t as = 0, aph = 0, rs = 0, rph = 0, issued_a = 0, issued_r = 0;
+            uint32_t as = 0, aph = 0, issued_a = 0;
             bool ok = true;
             for (long long u = pair; u < units && ok; u += npairs) {
                 const Unit un = decode(a, u);
@@ -564,8 +570,32 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                         tc::tma_load_2d(sm.a[as] + 32 * w * KS, &maps.hi, ks * KS, arow + A_BOX * w, &sm.afull[as]);
                     ++issued_a;
                     advance<STAGES>(as, aph);
+                }
+            }
+            // no TMA write may still be landing in shared memory when the CTA exits: wait for
+            // the last loads issued into every slot. A stages of CTA 1 complete on its local
+            // barrier; CTA 0's also need CTA 1's forward, so CTA 0 waits for its own bytes only
+            // through the phases it can observe (all its issued phases complete on the normal
+            // path; after an abort the bounded wait ends).
+            int no_abort = 0;
+            for (uint32_t back = 1; back <= STAGES && back <= issued_a; ++back) {
+                const uint32_t slot = (as + STAGES - back) % STAGES, par = back > as ? (aph ^ 1u) : aph;
+                if (!tc::mbar_wait(&sm.afull[slot], par, &no_abort)) fail(a, sm, 8);
+            }
+        }
+    } else if (warp == 14) {
+        // ---------------- raw loader: j one-hot rows and trait digit rows ----------------
+        // gated only by the B producers' consumption, so it runs up to RSTAGES stages ahead
+        // of them (the j rows come from DRAM once per pair tile)
+        if (lane == 0) {
+            uint32_t rs = 0, rph = 0, issued_r = 0;
+            bool ok = true;
+            for (long long u = pair; u < units && ok; u += npairs) {
+                const Unit un = decode(a, u);
+                if (un.skip) continue;
+                for (int ks = 0; ks < nks; ++ks) {
                     if (!tc::mbar_wait(&sm.raw_empty[rs], rph ^ 1u, abort)) {
-                        fail(a, sm, 7);
+                        fail(a, sm, 10);
                         ok = false;
                         break;
                     }
@@ -577,19 +607,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     advance<RSTAGES>(rs, rph);
                 }
             }
-            // no TMA write may still be landing in shared memory when the CTA exits: wait for
-            // the last loads issued into every ring slot. The raw stages complete on local
-            // barriers; A stages of CTA 1 do too, CTA 0's also need CTA 1's forward, so CTA 0
-            // waits for its own bytes only through the phases it can observe (all its
-            // issued phases complete on the normal path; after an abort the bounded wait ends).
             int no_abort = 0;
-            for (uint32_t back = 1; back <= STAGES && back <= issued_a; ++back) {
-                const uint32_t slot = (as + STAGES - back) % STAGES, par = back > as ? (aph ^ 1u) : aph;
-                if (!tc::mbar_wait(&sm.afull[slot], par, &no_abort)) fail(a, sm, 8);
-            }
             for (uint32_t back = 1; back <= RSTAGES && back <= issued_r; ++back) {
                 const uint32_t slot = (rs + RSTAGES - back) % RSTAGES, par = back > rs ? (rph ^ 1u) : rph;
-                if (!tc::mbar_wait(&sm.raw_full[slot], par, &no_abort)) fail(a, sm, 8);
+                if (!tc::mbar_wait(&sm.raw_full[slot], par, &no_abort)) fail(a, sm, 11);
             }
         }
     } else if (lane == 0 && rank == 1) {
@@ -660,8 +681,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         tc::tc_fence_after();
         tc::tmem_dealloc_pair(tmem, TMEM_COLS);
     }
-    for (int w = threadIdx.x; w < 2 * a.ntraits; w += blockDim.x)
-        if (smax[w]) atomicMax(w < a.ntraits ? &a.maxf[w] : &a.maxf2[w - a.ntraits], smax[w]);
+    if (smax_local)
+        for (int w = threadIdx.x; w < 2 * a.ntraits; w += blockDim.x)
+            if (smax[w]) atomicMax(w < a.ntraits ? &a.maxf[w] : &a.maxf2[w - a.ntraits], smax[w]);
 }
 
 }  // namespace mma
@@ -713,7 +735,7 @@ cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStr
 {
     // more than half of the SM's shared memory: one CTA per SM, which owns all 512 TMEM
     // columns; the tail holds the per-CTA maxima. CTAs run in clusters of two (the pair MMA).
-    const size_t smem = sizeof(mma::Smem) + 1024 + 8 * (size_t)a.ntraits;
+    const size_t smem = sizeof(mma::Smem) + 1024 + smax_bytes(a.ntraits);
     static_assert(sizeof(mma::Smem) + 1024 > 116 * 1024, "one CTA per SM");
     cudaError_t e = cudaFuncSetAttribute(mma::k_scan_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

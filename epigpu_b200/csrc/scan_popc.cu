@@ -115,9 +115,14 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
     Smem &sm = *reinterpret_cast<Smem *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nstages = a.Wp / KW;
-    // per-CTA maxima of F and F2 per trait (flushed to global memory once, at the end)
+    // maxima of F and F2 per trait: per CTA in shared memory (flushed to global memory once,
+    // at the end) up to SMAX_TRAITS traits, else the global maxima directly
+    const bool smax_local = a.ntraits <= SMAX_TRAITS;
     unsigned int *smax = reinterpret_cast<unsigned int *>(smem_raw + sizeof(Smem));
-    for (int w = tid; w < 2 * a.ntraits; w += NT) smax[w] = 0u;
+    if (smax_local)
+        for (int w = tid; w < 2 * a.ntraits; w += NT) smax[w] = 0u;
+    unsigned int *const mxf = smax_local ? smax : a.maxf;
+    unsigned int *const mxf2 = smax_local ? smax + a.ntraits : a.maxf2;
 
     for (;;) {
         if (tid == 0) sm.tile = (long long)atomicAdd(&a.counters[1], 1ull);
@@ -245,14 +250,15 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a)
                 const bool hit = valid && report && is_hit(a, s);
                 if (RAW) emit_row(a, hit, bd.start1 + gi, bd.start2 + gj, s);
                 else emit_hit(a, hit, bd.start1 + gi, bd.start2 + gj, s, t, b);
-                fold_max(&smax[t], valid, s.F);
-                if (a.test_int) fold_max(&smax[a.ntraits + t], valid, s.F2);
+                fold_max(&mxf[t], valid, s.F);
+                if (a.test_int) fold_max(&mxf2[t], valid, s.F2);
             }
         }
     }
     __syncthreads();
-    for (int w = tid; w < 2 * a.ntraits; w += NT)
-        if (smax[w]) atomicMax(w < a.ntraits ? &a.maxf[w] : &a.maxf2[w - a.ntraits], smax[w]);
+    if (smax_local)
+        for (int w = tid; w < 2 * a.ntraits; w += NT)
+            if (smax[w]) atomicMax(w < a.ntraits ? &a.maxf[w] : &a.maxf2[w - a.ntraits], smax[w]);
 }
 
 }  // namespace popc
@@ -264,7 +270,7 @@ int popc_words_multiple() { return popc::KW; }
 
 cudaError_t launch_popc(const ScanArgs &a, int grid, cudaStream_t stream)
 {
-    const size_t smem = sizeof(popc::Smem) + 8 * (size_t)a.ntraits;
+    const size_t smem = sizeof(popc::Smem) + smax_bytes(a.ntraits);
     cudaError_t e =
         cudaFuncSetAttribute(popc::k_scan_popc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
