@@ -43,8 +43,8 @@
 //   warp 12       CTA 0: MMA issuer (one thread): 4 pair MMAs per stage; CTA 1: forwards the
 //                 completion of its own A stages to CTA 0. Both: TMEM allocation (pair form)
 //   warps 0-3, 8-11  epilogue, two warps per TMEM lane quarter, three j rounds each
-// Handshakes: CTA 0's full / afull / acc_empty barriers also count arrivals from CTA 1; the
-// MMA's commits arrive on both CTAs' empty and acc_full barriers (multicast). TMEM (512
+// Handshakes: CTA 0's bfull / afull / acc_empty barriers also count arrivals from CTA 1; the
+// MMA's commits arrive on both CTAs' aempty, bempty and acc_full barriers (multicast). TMEM (512
 // columns per CTA): accumulators at [0, 256) and [256, 512). All waits are bounded
 // (tc_ptx.cuh); a timeout sets counters[2] and every role leaves its loop; the CTAs meet in
 // a cluster barrier before the TMEM is released.
@@ -67,8 +67,20 @@ constexpr int N = 256;         // MMA width (pair MMAs take multiples of 32); co
 constexpr int NH = N / 2;      // B columns held by each CTA
 constexpr int M = 256;         // MMA height over the pair
 constexpr int KS = 128;        // individuals per pipeline stage
-constexpr int STAGES = 5;      // operand ring (A and B of a stage share the slot index)
-constexpr int RSTAGES = 10;    // raw ring (smem, TMA)
+// operand rings: A stages come by TMA from L2 / DRAM and need the deeper ring; B stages are
+// built from raw rows already in shared memory
+#ifndef EPI_MMA_ASTAGES
+#define EPI_MMA_ASTAGES 7
+#endif
+#ifndef EPI_MMA_BSTAGES
+#define EPI_MMA_BSTAGES 3
+#endif
+constexpr int ASTAGES = EPI_MMA_ASTAGES;
+constexpr int BSTAGES = EPI_MMA_BSTAGES;
+#ifndef EPI_MMA_RSTAGES
+#define EPI_MMA_RSTAGES 10
+#endif
+constexpr int RSTAGES = EPI_MMA_RSTAGES;  // raw ring (smem, TMA)
 constexpr int ND = 7;          // digit rows per trait: w, Y digits (3), E digits (3)
 constexpr int ROUNDS = (TJ + 2) / 3;  // j rounds of the epilogue (3 j-SNPs per round)
 constexpr uint32_t ACC_COL1 = N;
@@ -91,13 +103,14 @@ static_assert(NCOL - NH == 7 * TJ && NH == 8 * TJ, "B split: CTA 0 types 0-7, CT
 static_assert(2 * N <= (int)TMEM_COLS && ROUNDS % 2 == 0, "TMEM layout / epilogue split");
 
 struct Smem {
-    uint8_t a[STAGES][A_STAGE];
-    uint8_t b[STAGES][B_STAGE];
+    uint8_t a[ASTAGES][A_STAGE];
+    uint8_t b[BSTAGES][B_STAGE];
     uint8_t raw[RSTAGES][RAW_STAGE];
-    // full: B halves built (CTA 0: 4 local + 4 remote producer warps); afull: A stages landed
-    // (CTA 0: own TMA + CTA 1's forward; CTA 1: own TMA); empty: MMAs of the slot done (both)
-    uint64_t full[STAGES], empty[STAGES], afull[STAGES], raw_full[RSTAGES], raw_empty[RSTAGES],
-        acc_full[2], acc_empty[2], drain;
+    // bfull: B halves built (CTA 0: 4 local + 4 remote producer warps); afull: A stages landed
+    // (CTA 0: own TMA + CTA 1's forward; CTA 1: own TMA); aempty / bempty: the MMAs reading
+    // the slot are done (both CTAs)
+    uint64_t afull[ASTAGES], aempty[ASTAGES], bfull[BSTAGES], bempty[BSTAGES], raw_full[RSTAGES],
+        raw_empty[RSTAGES], acc_full[2], acc_empty[2], drain;
     uint32_t tmem_base;
     int abort;
 };
@@ -220,13 +233,13 @@ __device__ __forceinline__ PairStat pair_stat_exact(const int n[9], const double
 // A pair whose screened F and F2 are clearly below every threshold and below the running
 // maxima cannot be a hit or a new maximum, and keeps these values; every other pair is
 // recomputed by pair_stat_exact.
-__device__ __forceinline__ void pair_stat_f32(const int n[9], const double si[9], float sc, float Q, bool want_int,
+__device__ __forceinline__ void pair_stat_f32(const int n[9], const float sd[9], float sc, float Q, bool want_int,
                                               float &F, float &F2)
 {
     float N = 0.0f, St = 0.0f, nfac = 0.0f, sf[9];
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
-        sf[c] = (float)si[c] * sc;
+        sf[c] = sd[c] * sc;
         N += (float)n[c];
         St += sf[c];
         nfac += n[c] > 0 ? 1.0f : 0.0f;
@@ -293,7 +306,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
     }
     // CTA 1 holds B columns 128-255: its rows 112-127 (columns 240-255) stay zero
     if (rank == 1)
-        for (int w = threadIdx.x; w < STAGES * (NH - (NCOL - NH)) * 8; w += blockDim.x) {
+        for (int w = threadIdx.x; w < BSTAGES * (NH - (NCOL - NH)) * 8; w += blockDim.x) {
             const int st = w / ((NH - (NCOL - NH)) * 8), n = (NCOL - NH) + (w / 8) % (NH - (NCOL - NH)), c = w % 8;
             *reinterpret_cast<uint4 *>(sm.b[st] + (n >> 3) * 1024 + (n & 7) * 128 + c * 16) = make_uint4(0, 0, 0, 0);
         }
@@ -307,10 +320,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
     unsigned int *const mxf = smax_local ? smax : a.maxf;
     unsigned int *const mxf2 = smax_local ? smax + a.ntraits : a.maxf2;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < STAGES; ++s) {
-            tc::mbar_init(&sm.full[s], rank == 0 ? 8 : 1);
-            tc::mbar_init(&sm.empty[s], 1);
+        for (int s = 0; s < ASTAGES; ++s) {
             tc::mbar_init(&sm.afull[s], rank == 0 ? 2 : 1);
+            tc::mbar_init(&sm.aempty[s], 1);
+        }
+        for (int s = 0; s < BSTAGES; ++s) {
+            tc::mbar_init(&sm.bfull[s], rank == 0 ? 8 : 1);
+            tc::mbar_init(&sm.bempty[s], 1);
         }
         for (int r = 0; r < RSTAGES; ++r) {
             tc::mbar_init(&sm.raw_full[r], 1);
@@ -340,7 +356,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             const Unit un = decode(a, u);
             if (un.skip) continue;
             for (int ks = 0; ks < nks; ++ks) {
-                if (!tc::mbar_wait(&sm.raw_full[rs], rph, abort) || !tc::mbar_wait(&sm.empty[stage], phase ^ 1u, abort)) {
+                if (!tc::mbar_wait(&sm.raw_full[rs], rph, abort) || !tc::mbar_wait(&sm.bempty[stage], phase ^ 1u, abort)) {
                     fail(a, sm, 2);
                     ok = false;
                     break;
@@ -402,10 +418,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 __syncwarp();
                 if (lane == 0) {
                     tc::mbar_arrive(&sm.raw_empty[rs]);
-                    if (rank == 0) tc::mbar_arrive(&sm.full[stage]);
-                    else tc::mbar_arrive_remote(&sm.full[stage], 0);
+                    if (rank == 0) tc::mbar_arrive(&sm.bfull[stage]);
+                    else tc::mbar_arrive_remote(&sm.bfull[stage], 0);
                 }
-                advance<STAGES>(stage, phase);
+                advance<BSTAGES>(stage, phase);
                 advance<RSTAGES>(rs, rph);
             }
         }
@@ -471,8 +487,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     // deliver them: relative row 0 = own (a = ga), 1 = r1 (a = ga+1), 2 = r2
                     // (a = ga+2, mod 3). F and F2 do not depend on the order of the rows; only
                     // the count dump below maps them back to a.
-                    int n[9];
-                    double si[9];  // digit sums as exact integers
+                    int n[9], g1[9], g2[9], g3[9];  // counts and the three digit sums per cell
 #pragma unroll
                     for (int b = 0; b < 3; ++b) {
                         const uint32_t c0[3] = {sel3(v[4 * b], ga), r1[4 * b], r2[4 * b]};
@@ -482,10 +497,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
 #pragma unroll
                         for (int r = 0; r < 3; ++r) {
                             n[3 * r + b] = (int)c0[r];
-                            si[3 * r + b] =
-                                fma(65536.0, (double)(int)c3[r], fma(256.0, (double)(int)c2[r], (double)(int)c1[r]));
+                            g1[3 * r + b] = (int)c1[r];
+                            g2[3 * r + b] = (int)c2[r];
+                            g3[3 * r + b] = (int)c3[r];
                         }
                     }
+                    // the screen's sums in FP32: up to 131,072 individuals each digit sum is
+                    // below 2^24 in magnitude, so the conversions are exact and the two fmas
+                    // round once each; beyond, the conversions round too (relative 2^-24, far
+                    // inside the screen's margin)
+                    float sfd[9];
+#pragma unroll
+                    for (int c = 0; c < 9; ++c)
+                        sfd[c] = fmaf(65536.0f, (float)g3[c], fmaf(256.0f, (float)g2[c], (float)g1[c]));
                     int npair = 0;
 #pragma unroll
                     for (int c = 0; c < 9; ++c) npair += n[c];
@@ -499,10 +523,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     }
                     const double Q = fma(qcen, (double)npair, pki) - fma(qstep, (double)em, rmj);
                     float Ff, F2f;
-                    pair_stat_f32(n, si, scf, (float)Q, a.test_int != 0, Ff, F2f);
+                    pair_stat_f32(n, sfd, scf, (float)Q, a.test_int != 0, Ff, F2f);
                     const bool exact = dumping || npair < 256 || !(Ff <= t1c) || !(Ff <= screen_lo(fmx_f)) ||
                                        (a.test_int && (!(F2f <= t2c) || !(F2f <= screen_lo(f2mx_f))));
                     if (exact) {
+                        double si[9];  // digit sums as exact integers
+#pragma unroll
+                        for (int c = 0; c < 9; ++c)
+                            si[c] = fma(65536.0, (double)g3[c], fma(256.0, (double)g2[c], (double)g1[c]));
                         s = pair_stat_exact(n, si, sc, Q, a.test_int != 0);
                     } else {
                         // below every threshold and both running maxima by more than the margin
@@ -559,7 +587,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 if (un.skip) continue;
                 const int arow = 3 * (un.bd.start1 + un.i0 + TI * (int)rank);
                 for (int ks = 0; ks < nks; ++ks) {
-                    if (!tc::mbar_wait(&sm.empty[as], aph ^ 1u, abort)) {
+                    if (!tc::mbar_wait(&sm.aempty[as], aph ^ 1u, abort)) {
                         fail(a, sm, 7);
                         ok = false;
                         break;
@@ -569,7 +597,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     for (int w = 0; w < 4; ++w)
                         tc::tma_load_2d(sm.a[as] + 32 * w * KS, &maps.hi, ks * KS, arow + A_BOX * w, &sm.afull[as]);
                     ++issued_a;
-                    advance<STAGES>(as, aph);
+                    advance<ASTAGES>(as, aph);
                 }
             }
             // no TMA write may still be landing in shared memory when the CTA exits: wait for
@@ -578,8 +606,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             // through the phases it can observe (all its issued phases complete on the normal
             // path; after an abort the bounded wait ends).
             int no_abort = 0;
-            for (uint32_t back = 1; back <= STAGES && back <= issued_a; ++back) {
-                const uint32_t slot = (as + STAGES - back) % STAGES, par = back > as ? (aph ^ 1u) : aph;
+            for (uint32_t back = 1; back <= ASTAGES && back <= issued_a; ++back) {
+                const uint32_t slot = (as + ASTAGES - back) % ASTAGES, par = back > as ? (aph ^ 1u) : aph;
                 if (!tc::mbar_wait(&sm.afull[slot], par, &no_abort)) fail(a, sm, 8);
             }
         }
@@ -628,12 +656,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                     break;
                 }
                 tc::mbar_arrive_remote(&sm.afull[as], 0);
-                advance<STAGES>(as, aph);
+                advance<ASTAGES>(as, aph);
             }
         }
     } else if (lane == 0) {
         // ---------------- MMA issuer (CTA 0, warp 12) ----------------
-        uint32_t stage = 0, phase = 0, accph[2] = {0u, 0u};
+        uint32_t as = 0, aph = 0, bs = 0, bph = 0, accph[2] = {0u, 0u};
         int buf = 0;
         bool ok = true;
         for (long long u = pair; u < units && ok; u += npairs) {
@@ -646,20 +674,22 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             tc::tc_fence_after();
             const uint32_t d = tmem + acc_col(buf);
             for (int ks = 0; ks < nks; ++ks) {
-                if (!tc::mbar_wait_cluster(&sm.full[stage], phase, abort) ||
-                    !tc::mbar_wait_cluster(&sm.afull[stage], phase, abort)) {
+                if (!tc::mbar_wait_cluster(&sm.bfull[bs], bph, abort) ||
+                    !tc::mbar_wait_cluster(&sm.afull[as], aph, abort)) {
                     fail(a, sm, 5);
                     ok = false;
                     break;
                 }
                 tc::tc_fence_after();
-                const uint32_t asb = tc::smem_u32(sm.a[stage]), bsb = tc::smem_u32(sm.b[stage]);
+                const uint32_t asb = tc::smem_u32(sm.a[as]), bsb = tc::smem_u32(sm.b[bs]);
 #pragma unroll
                 for (int kk = 0; kk < KS / 32; ++kk)
                     tc::mma_i8_pair(d, tc::smem_desc_sw128(asb + 32 * kk), tc::smem_desc_sw128(bsb + 32 * kk), IDESC,
                                     (ks | kk) != 0);
-                tc::mma_commit_pair_mc(&sm.empty[stage], 0x3);
-                advance<STAGES>(stage, phase);
+                tc::mma_commit_pair_mc(&sm.aempty[as], 0x3);
+                tc::mma_commit_pair_mc(&sm.bempty[bs], 0x3);
+                advance<ASTAGES>(as, aph);
+                advance<BSTAGES>(bs, bph);
             }
             if (!ok) break;
             tc::mma_commit_pair_mc(&sm.acc_full[buf], 0x3);
