@@ -152,6 +152,12 @@ __device__ __forceinline__ uint32_t sel3(const uint32_t v[4], int idx)
     return idx == 0 ? v[0] : (idx == 1 ? v[1] : v[2]);
 }
 
+template <class T>
+__device__ __forceinline__ T pick3(T x0, T x1, T x2, int idx)
+{
+    return idx == 0 ? x0 : (idx == 1 ? x1 : x2);
+}
+
 // 1/x for x > 0: single-precision seed (__frcp_rn) refined by one Newton step in FP64,
 // e = 1 - x r, r' = r + r e, which squares the seed's relative error (2^-24 -> ~2^-48).
 __device__ __forceinline__ double rcp_d(double x)
@@ -252,7 +258,15 @@ __device__ __forceinline__ void pair_stat_f32(const int n[9], const float sd[9],
         const float d = mc[c] - m;
         SSB = fmaf((float)n[c] * d, d, SSB);
     }
-    const float SSW = (Q - St * m) - SSB;
+    const float SSY = Q - St * m;  // sum of squares about the pair's mean
+    const float SSW = SSY - SSB;
+    // SSW carries an absolute error of a few ulps of SSY; while SSW > 1e-3 SSY its relative
+    // error stays below ~3e-4, inside the margin. A closer fit (or a negative SSW from
+    // rounding) goes to the exact path: NaN fails every screen comparison.
+    if (!(SSW > 1e-3f * SSY)) {
+        F = F2 = __int_as_float(0x7fc00000);
+        return;
+    }
     const float d1 = nfac - 1.0f, d2 = N - nfac;
     F = (SSB * d2) / (SSW * d1);
     F2 = 0.0f;
@@ -453,6 +467,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             const bool report = a.report_trait < 0 || a.report_trait == t;
             const bool dumping = t == a.report_trait && (a.dump_counts || a.dump_F);
             const float t1c = screen_lo(a.t1), t2c = screen_lo(a.t2), scf = (float)sc;
+            const float qcenf = (float)qcen, qstepf = (float)qstep, pkif = (float)pki;
             unsigned int fmx = 0u, f2mx = 0u;  // this thread's largest F, F2 of the tile (encoded)
             // screen against the CTA's maxima so far (exact values, a lower bound of the final
             // maxima): a pair that can raise a maximum always takes the exact path
@@ -472,67 +487,60 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 for (int ty = 0; ty < NTYPE; ++ty)
                     tc::tmem_ld4(acc + ty * TJ + jb, v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
                 tc::tmem_wait_ld();
-                // rows (ii, a') for my j-SNP jb + ga: own row directly, the others by shuffle
-                uint32_t r1[NTYPE], r2[NTYPE];
+                // this lane's accumulator row (SNP i, genotype ga) folded per column c of the round
+                // (j-SNP jb + c): three counts, three FP32 phenotype sums and the FP32 sum of E.
+                // Up to 131,072 individuals every digit sum is below 2^24 in magnitude, so the
+                // conversions are exact and the two fmas round once each (beyond, the conversions
+                // round too: relative 2^-24, far inside the screen's margin).
+                int cn[3][3];
+                float cs[3][3], ce[3];
 #pragma unroll
-                for (int ty = 0; ty < NTYPE; ++ty) {
-                    r1[ty] = __shfl_sync(0xffffffffu, sel3(v[ty], (ga + 2) % 3), tbase + (ga + 1) % 3);
-                    r2[ty] = __shfl_sync(0xffffffffu, sel3(v[ty], (ga + 1) % 3), tbase + (ga + 2) % 3);
+                for (int c = 0; c < 3; ++c) {
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) {
+                        cn[c][b] = (int)v[4 * b][c];
+                        cs[c][b] = fmaf(65536.0f, (float)(int)v[4 * b + 3][c],
+                                        fmaf(256.0f, (float)(int)v[4 * b + 2][c], (float)(int)v[4 * b + 1][c]));
+                    }
+                    ce[c] = fmaf(65536.0f, (float)(int)v[NTY + 2][c],
+                                 fmaf(256.0f, (float)(int)v[NTY + 1][c], (float)(int)v[NTY][c]));
                 }
+                // the pair (SNP i, j-SNP jb + ga) is this lane's: its own row directly, the rows of
+                // the triplet's other two lanes by shuffle, each lane offering the column its reader
+                // needs (the lane of genotype ga+1 offers its column (ga+1)+2 = ga, mod 3). Cells
+                // row-major in this relative row order (own, ga+1, ga+2): F and F2 do not depend
+                // on the order of the rows; only the count dump maps them back to genotypes.
+                const int s1 = tbase + (ga + 1) % 3, s2 = tbase + (ga + 2) % 3;
+                const int o1 = (ga + 2) % 3, o2 = (ga + 1) % 3;  // the columns this lane offers
+                int n[9];
+                float sfd[9];
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    n[b] = pick3(cn[0][b], cn[1][b], cn[2][b], ga);
+                    n[3 + b] = __shfl_sync(0xffffffffu, pick3(cn[0][b], cn[1][b], cn[2][b], o1), s1);
+                    n[6 + b] = __shfl_sync(0xffffffffu, pick3(cn[0][b], cn[1][b], cn[2][b], o2), s2);
+                    sfd[b] = pick3(cs[0][b], cs[1][b], cs[2][b], ga);
+                    sfd[3 + b] = __shfl_sync(0xffffffffu, pick3(cs[0][b], cs[1][b], cs[2][b], o1), s1);
+                    sfd[6 + b] = __shfl_sync(0xffffffffu, pick3(cs[0][b], cs[1][b], cs[2][b], o2), s2);
+                }
+                // E sum over individuals known at i (the three rows) and missing at j
+                const float emf = pick3(ce[0], ce[1], ce[2], ga) +
+                                  __shfl_sync(0xffffffffu, pick3(ce[0], ce[1], ce[2], o1), s1) +
+                                  __shfl_sync(0xffffffffu, pick3(ce[0], ce[1], ce[2], o2), s2);
                 PairStat s;
                 s.nfac = s.d1 = s.d2 = 0;
                 s.F = s.F2 = 0.0;
+                int npair = 0;
+                bool exact = false;
                 if (valid) {
-                    // cells row-major with the genotype rows of SNP i in the order the shuffles
-                    // deliver them: relative row 0 = own (a = ga), 1 = r1 (a = ga+1), 2 = r2
-                    // (a = ga+2, mod 3). F and F2 do not depend on the order of the rows; only
-                    // the count dump below maps them back to a.
-                    int n[9], g1[9], g2[9], g3[9];  // counts and the three digit sums per cell
-#pragma unroll
-                    for (int b = 0; b < 3; ++b) {
-                        const uint32_t c0[3] = {sel3(v[4 * b], ga), r1[4 * b], r2[4 * b]};
-                        const uint32_t c1[3] = {sel3(v[4 * b + 1], ga), r1[4 * b + 1], r2[4 * b + 1]};
-                        const uint32_t c2[3] = {sel3(v[4 * b + 2], ga), r1[4 * b + 2], r2[4 * b + 2]};
-                        const uint32_t c3[3] = {sel3(v[4 * b + 3], ga), r1[4 * b + 3], r2[4 * b + 3]};
-#pragma unroll
-                        for (int r = 0; r < 3; ++r) {
-                            n[3 * r + b] = (int)c0[r];
-                            g1[3 * r + b] = (int)c1[r];
-                            g2[3 * r + b] = (int)c2[r];
-                            g3[3 * r + b] = (int)c3[r];
-                        }
-                    }
-                    // the screen's sums in FP32: up to 131,072 individuals each digit sum is
-                    // below 2^24 in magnitude, so the conversions are exact and the two fmas
-                    // round once each; beyond, the conversions round too (relative 2^-24, far
-                    // inside the screen's margin)
-                    float sfd[9];
-#pragma unroll
-                    for (int c = 0; c < 9; ++c)
-                        sfd[c] = fmaf(65536.0f, (float)g3[c], fmaf(256.0f, (float)g2[c], (float)g1[c]));
-                    int npair = 0;
 #pragma unroll
                     for (int c = 0; c < 9; ++c) npair += n[c];
-                    // E digit sums over individuals known at i (rows a = 0..2) and missing at j
-                    long long em = 0;
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        const long long sd = (long long)(int)sel3(v[NTY + d], ga) + (long long)(int)r1[NTY + d] +
-                                             (long long)(int)r2[NTY + d];
-                        em += sd * (1LL << (8 * d));
-                    }
-                    const double Q = fma(qcen, (double)npair, pki) - fma(qstep, (double)em, rmj);
+                    const float Qf = fmaf(qcenf, (float)npair, pkif) - fmaf(qstepf, emf, (float)rmj);
                     float Ff, F2f;
-                    pair_stat_f32(n, sfd, scf, (float)Q, a.test_int != 0, Ff, F2f);
-                    const bool exact = dumping || npair < 256 || !(Ff <= t1c) || !(Ff <= screen_lo(fmx_f)) ||
-                                       (a.test_int && (!(F2f <= t2c) || !(F2f <= screen_lo(f2mx_f))));
-                    if (exact) {
-                        double si[9];  // digit sums as exact integers
-#pragma unroll
-                        for (int c = 0; c < 9; ++c)
-                            si[c] = fma(65536.0, (double)g3[c], fma(256.0, (double)g2[c], (double)g1[c]));
-                        s = pair_stat_exact(n, si, sc, Q, a.test_int != 0);
-                    } else {
+                    pair_stat_f32(n, sfd, scf, Qf, a.test_int != 0, Ff, F2f);
+                    exact = dumping || npair < 256 || !(Ff <= t1c) || !(Ff <= screen_lo(fmx_f)) ||
+                            (a.test_int && (!(F2f <= t2c) || !(F2f <= screen_lo(f2mx_f))));
+                    if (!exact) {
                         // below every threshold and both running maxima by more than the margin
                         int nfac = 0;
 #pragma unroll
@@ -543,17 +551,54 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                         s.F = Ff;
                         s.F2 = F2f;
                     }
-                    if (dumping) {
-                        const size_t o = (size_t)di * un.bd.size2 + dj;
-                        if (a.dump_counts)
+                }
+                if (__any_sync(0xffffffffu, exact)) {
+                    // rare (pairs near a threshold or a running maximum, count dumps, small
+                    // blocks): the exact digit sums of every cell, gathered again from the
+                    // accumulator (still in TMEM until this warp releases it)
 #pragma unroll
-                            for (int c = 0; c < 9; ++c)  // relative row c/3 is genotype (ga + c/3) mod 3
-                                a.dump_counts[9 * o + 3 * ((ga + c / 3) % 3) + c % 3] = n[c];
-                        if (a.dump_F) a.dump_F[o] = (float)s.F;
-                        if (a.dump_F2) a.dump_F2[o] = (float)s.F2;
-                        if (a.dump_df1) a.dump_df1[o] = s.d1;
-                        if (a.dump_df2) a.dump_df2[o] = s.d2;
+                    for (int ty = 0; ty < NTYPE; ++ty)
+                        tc::tmem_ld4(acc + ty * TJ + jb, v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
+                    tc::tmem_wait_ld();
+                    uint32_t r1[NTYPE], r2[NTYPE];
+#pragma unroll
+                    for (int ty = 0; ty < NTYPE; ++ty) {
+                        r1[ty] = __shfl_sync(0xffffffffu, sel3(v[ty], o1), s1);
+                        r2[ty] = __shfl_sync(0xffffffffu, sel3(v[ty], o2), s2);
                     }
+                    if (exact) {
+                        double si[9];  // digit sums as exact integers
+#pragma unroll
+                        for (int b = 0; b < 3; ++b) {
+                            const uint32_t c1[3] = {sel3(v[4 * b + 1], ga), r1[4 * b + 1], r2[4 * b + 1]};
+                            const uint32_t c2[3] = {sel3(v[4 * b + 2], ga), r1[4 * b + 2], r2[4 * b + 2]};
+                            const uint32_t c3[3] = {sel3(v[4 * b + 3], ga), r1[4 * b + 3], r2[4 * b + 3]};
+#pragma unroll
+                            for (int r = 0; r < 3; ++r)
+                                si[3 * r + b] = fma(65536.0, (double)(int)c3[r],
+                                                    fma(256.0, (double)(int)c2[r], (double)(int)c1[r]));
+                        }
+                        long long em = 0;
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            const long long sd = (long long)(int)sel3(v[NTY + d], ga) + (long long)(int)r1[NTY + d] +
+                                                 (long long)(int)r2[NTY + d];
+                            em += sd * (1LL << (8 * d));
+                        }
+                        const double Q = fma(qcen, (double)npair, pki) - fma(qstep, (double)em, rmj);
+                        s = pair_stat_exact(n, si, sc, Q, a.test_int != 0);
+                    }
+                }
+                if (valid && dumping) {
+                    const size_t o = (size_t)di * un.bd.size2 + dj;
+                    if (a.dump_counts)
+#pragma unroll
+                        for (int c = 0; c < 9; ++c)  // relative row c/3 is genotype (ga + c/3) mod 3
+                            a.dump_counts[9 * o + 3 * ((ga + c / 3) % 3) + c % 3] = n[c];
+                    if (a.dump_F) a.dump_F[o] = (float)s.F;
+                    if (a.dump_F2) a.dump_F2[o] = (float)s.F2;
+                    if (a.dump_df1) a.dump_df1[o] = s.d1;
+                    if (a.dump_df2) a.dump_df2[o] = s.d2;
                 }
                 const bool hit = valid && report && is_hit(a, s);
                 emit_hit(a, hit, un.bd.start1 + di, un.bd.start2 + dj, s, t, un.block);
