@@ -131,6 +131,25 @@ struct PairStat {
 //   F = (SSB/d1) / ((SSY-SSB)/d2);  4 df: row/column means from raw sums (:466-467),
 //   SSI = sum_c n_c (m_ab - r_a - c_b + m)^2, F2 = (SSI/4) / MSW.
 // d1 == 0 gives SSB == 0 and F = 0/0 = NaN (never a hit).
+//
+// Resolution floor: SSW = SSY - SSB cancels when the pair's cells explain nearly all of the
+// variance, and once SSW falls below the rounding error of the sums it came from, its value
+// (and sign) is noise. The caller states that error as a fraction of SSY (ssw_floor); below
+// it SSW is taken as ssw_floor * SSY, so F is a lower bound of the true F (which is larger
+// still) and such a pair stays a hit; the relative error in F stays within the documented
+// 1e-5 * SSY / SSW. NaN inputs stay NaN.
+__device__ __forceinline__ double ssw_floored(double SSY, double SSB, double ssw_floor)
+{
+    const double SSW = SSY - SSB;
+    return SSW < ssw_floor * SSY ? ssw_floor * SSY : SSW;
+}
+
+// floor for sums accumulated in FP32 over the individuals (the plain form)
+constexpr double SSW_FLOOR_F32 = 1e-5;
+// floor for the tensor form's exact integer sums (its Q carries the doubly-missing residual
+// approximation, at most ~1e-8 of SSY)
+constexpr double SSW_FLOOR_EXACT = 1e-7;
+
 __device__ __forceinline__ PairStat pair_stat(const int n[9], const double S[9], double Qv, bool want_int)
 {
     PairStat r;
@@ -157,7 +176,7 @@ __device__ __forceinline__ PairStat pair_stat(const int n[9], const double S[9],
     r.nfac = nfac;
     r.d1 = nfac - 1;
     r.d2 = N - nfac;
-    const double MSW = (SSY - SSB) / (double)r.d2;
+    const double MSW = ssw_floored(SSY, SSB, SSW_FLOOR_F32) / (double)r.d2;
     r.F = (SSB / (double)r.d1) / MSW;
     r.F2 = 0.0;
     if (want_int) {

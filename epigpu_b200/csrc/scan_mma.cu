@@ -22,7 +22,8 @@
 // same individuals, taken as RM_j (r summed over all individuals missing at j, FP64, per
 // SNP). The one approximation: the residuals of individuals missing at both SNPs are counted
 // in RM_j, an error of at most qstep / 2 per such individual (qstep = max(ytilde^2) / 2^24).
-// The epilogue forms SSB / SSI / F / F2 in FP64.
+// The epilogue screens F and F2 in FP32 from the exact integer cells and forms SSB / SSI /
+// F / F2 in FP64 for every pair that could be a hit or a new maximum.
 //
 // The GEMM runs on a CTA pair (a cluster of two CTAs on two SMs, tcgen05 cta_group::2): one
 // MMA of M = 256 rows (each CTA's 40 i-SNPs, 3 genotype rows each, in its own shared memory)
@@ -204,7 +205,7 @@ __device__ __forceinline__ PairStat pair_stat_exact(const int n[9], const double
             SSB = fma((double)n[c] * d, d, SSB);
         }
     }
-    const double SSW = (Q - St * m) - SSB;
+    const double SSW = ssw_floored(Q - St * m, SSB, SSW_FLOOR_EXACT);
     r.nfac = nfac;
     r.d1 = nfac - 1;
     r.d2 = N - nfac;

@@ -72,3 +72,29 @@ def test_f_error_low_call_rate_individuals(gpu_ctx, form):
     for field in ("F", "F2"):
         ref, got = pb[field][tri], d[field][tri].astype(np.float64)
         assert parity.f_excess(got, ref, pb["df1"][tri], pb["df2"][tri], 1e-5).max() <= 1.0, field
+
+
+@pytest.mark.parametrize("form", [capi.FORM_POPC, capi.FORM_TENSOR], ids=["popc", "tensor"])
+@pytest.mark.parametrize("test", ["f", "i"])
+def test_near_perfect_fit_is_a_hit(gpu_ctx, form, test):
+    """A phenotype almost fully determined by one SNP pair's 3x3 genotype cells (noise 1e-6
+    of the cell effects): its F is ~1e12, SSW is a 1e-12 fraction of SSY, and a single-precision
+    screen of that pair would see only rounding noise in SSW. The pair must be a hit in both
+    forms, as in the FP64 oracle, and the hit lists must agree."""
+    nid, nsnp, pi, pj = 500, 24, 17, 5
+    codes = synth.genotype_codes(nid, nsnp, seed=71, miss=0.0)
+    rng = np.random.default_rng(72)
+    effect = rng.standard_normal((3, 3))
+    y = (effect[codes[pi], codes[pj]] + 1e-6 * rng.standard_normal(nid)).astype(np.float32)
+    t1 = synth.f_threshold(8, nid - 9, 1e-6)
+    t2 = synth.f_threshold(4, nid - 9, 1e-6)
+    blk = (0, nsnp, 0, nsnp)
+    gpu_ctx.load_packed(synth.pack(codes), nid)
+    gpu_ctx.set_phenotype(y)
+    hits, total, ex = gpu_ctx.scan([blk], capi.default_opts(test=test, t1=t1, t2=t2, form=form))
+    hb, tb, pb = oracles.oracle_scan_block(codes, y, blk, test=test, t1=t1, t2=t2, per_pair=True)
+    assert pb["F"][pi, pj] > 1e9
+    assert any(int(h["snp1"]) == pi and int(h["snp2"]) == pj for h in hits), "the fitted pair is missing"
+    excl = parity.near_threshold(pb, blk, t1, t2, test, 1e-4)
+    ok, msg = parity.compare_hit_lists(hits, hb, excl)
+    assert ok, msg
