@@ -52,6 +52,9 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <mutex>
+#include <vector>
+
 #include "epi_internal.cuh"
 #include "tc_ptx.cuh"
 
@@ -807,13 +810,26 @@ int mma_min_nid() { return 256; }
 int mma_max_nid() { return 1 << 24; }  // digit sums stay within int32
 int mma_stage_individuals() { return mma::KS; }
 
+// Launch shape per (device, dynamic shared memory size): the attribute set and the number
+// of co-resident clusters, queried once (the occupancy query costs far more than a small
+// scan's host work).
+struct MmaShape {
+    int device;
+    size_t smem;
+    int clusters;
+};
+
+static std::mutex g_shape_mu;
+static std::vector<MmaShape> g_shapes;
+
 cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream)
 {
     // more than half of the SM's shared memory: one CTA per SM, which owns all 512 TMEM
     // columns; the tail holds the per-CTA maxima. CTAs run in clusters of two (the pair MMA).
     const size_t smem = sizeof(mma::Smem) + 1024 + smax_bytes(a.ntraits);
     static_assert(sizeof(mma::Smem) + 1024 > 116 * 1024, "one CTA per SM");
-    cudaError_t e = cudaFuncSetAttribute(mma::k_scan_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
@@ -828,9 +844,21 @@ cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStr
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int clusters = 0;
-    e = cudaOccupancyMaxActiveClusters(&clusters, mma::k_scan_mma, &cfg);
-    if (e != cudaSuccess) return e;
-    if (clusters < 1) return cudaErrorInvalidConfiguration;
+    {
+        std::lock_guard<std::mutex> lock(g_shape_mu);
+        for (const MmaShape &sh : g_shapes)
+            if (sh.device == device && sh.smem == smem) clusters = sh.clusters;
+        if (clusters == 0) {
+            // the attribute admits the largest size any trait count asks for
+            e = cudaFuncSetAttribute(mma::k_scan_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(sizeof(mma::Smem) + 1024 + smax_bytes(SMAX_TRAITS)));
+            if (e != cudaSuccess) return e;
+            e = cudaOccupancyMaxActiveClusters(&clusters, mma::k_scan_mma, &cfg);
+            if (e != cudaSuccess) return e;
+            if (clusters < 1) return cudaErrorInvalidConfiguration;
+            g_shapes.push_back({device, smem, clusters});
+        }
+    }
     if (2 * clusters < (int)cfg.gridDim.x) cfg.gridDim.x = 2 * (unsigned)clusters;
     e = cudaLaunchKernelEx(&cfg, mma::k_scan_mma, a, maps);
     if (e != cudaSuccess) return e;
