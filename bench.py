@@ -229,10 +229,14 @@ def cpu_baseline(data, test, t1, t2, budget_s=12.0, min_m=200):
                                           nthreads=threads)
         return time.perf_counter() - t, m * (m - 1) // 2
 
-    dt, pairs = run(min_m)
-    rate = pairs / dt
-    m = int(min(data["nsnp"], max(min_m, (2 * rate * budget_s) ** 0.5)))
-    dt, pairs = run(m)
+    # small samples run below the threads' full rate (start-up), so the size is refined from
+    # each run until one takes at least half the budget
+    m = min_m
+    for _ in range(4):
+        dt, pairs = run(m)
+        if dt >= 0.5 * budget_s or m >= data["nsnp"]:
+            break
+        m = int(min(data["nsnp"], max(m + 1, (2 * pairs / dt * budget_s) ** 0.5)))
     return {"value": pairs / dt, "unit": "pairs/s", "cores": threads, "kind": "reference",
             "sample": "triangle of the first %d SNPs at N=%d (%d pairs, %s test), %.1f s" % (m, nid, pairs,
                                                                                          "8df+4df" if test == "i"
