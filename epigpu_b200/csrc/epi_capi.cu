@@ -99,9 +99,11 @@ static epi_status set_err(epi_ctx *ctx, epi_status s, const char *fmt, ...)
 #define CK(call)                                                                                      \
     do {                                                                                              \
         cudaError_t e_ = (call);                                                                      \
-        if (e_ != cudaSuccess)                                                                        \
+        if (e_ != cudaSuccess) {                                                                      \
+            cudaGetLastError(); /* a failed call must not surface again at the next launch check */  \
             return set_err(ctx, e_ == cudaErrorMemoryAllocation ? EPI_E_NOMEM : EPI_E_CUDA,          \
                            "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);      \
+        }                                                                                             \
     } while (0)
 
 template <class T>
@@ -530,11 +532,12 @@ epi_status launch_run(epi_ctx *ctx, ScanRun &r)
     ctx->last_launches = 0;
     ctx->last_form = r.form;
     if (r.ntiles > 0) {
-        const int grid = (int)std::min<int64_t>(r.ntiles, ctx->sm_count);
         if (r.form == EPI_FORM_TENSOR) {
-            CK(epi::launch_mma(r.args, ctx->maps, grid, ctx->stream));
+            // one CTA pair per unit (tile x trait) up to every SM
+            const int64_t units = r.ntiles * (int64_t)ctx->ntraits;
+            CK(epi::launch_mma(r.args, ctx->maps, (int)std::min<int64_t>(2 * units, ctx->sm_count), ctx->stream));
         } else {
-            CK(epi::launch_popc(r.args, grid, ctx->stream));
+            CK(epi::launch_popc(r.args, (int)std::min<int64_t>(r.ntiles, ctx->sm_count), ctx->stream));
         }
         ctx->last_launches = 1;
     }

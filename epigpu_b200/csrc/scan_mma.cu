@@ -52,6 +52,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -837,7 +838,8 @@ cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStr
     attr[0].val.clusterDim.x = 2;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3((unsigned)(grid & ~1), 1, 1);
+    // whole clusters of two: at least one, and never more than can be resident at once
+    cfg.gridDim = dim3((unsigned)std::max(2, (grid + 1) & ~1), 1, 1);
     cfg.blockDim = dim3(mma::NTHREADS, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
