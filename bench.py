@@ -116,6 +116,17 @@ def thresholds(nid):
     return synth.f_threshold(8, nid - 9, 1e-6), synth.f_threshold(4, nid - 9, 1e-6)
 
 
+def max_over_ranks(x, pg, device="cuda"):
+    """The largest x over all ranks, on every rank (x itself without a process group): a
+    multi-GPU time is the slowest rank's."""
+    if not pg:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 def block_pairs(b):
     s1, m1, s2, m2 = b
     gx = np.arange(m1, dtype=np.int64)
@@ -364,10 +375,7 @@ def main():
         e1.record(stream)
         barrier()
         dev_s = e0.elapsed_time(e1) / 1e3
-    if pg:
-        t = torch.tensor([dev_s], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        dev_s = float(t.item())
+    dev_s = max_over_ranks(dev_s, pg)
     value = pairs_step * args.steps * world / dev_s
     used_form = "tensor" if used == capi.FORM_TENSOR else "popc"
 
@@ -384,10 +392,7 @@ def main():
     e1.record(stream)
     barrier()
     e2e_s = e0.elapsed_time(e1) / 1e3
-    if pg:
-        t = torch.tensor([e2e_s], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, pg)
     h2d = gp.nbytes + y.nbytes + (valid.nbytes if valid is not None else 0)
     d2h = n * 32 + 64
 

@@ -40,3 +40,40 @@ def test_reference_arm_other_ranks_print_nothing():
              "--warmup", "1")
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def _rank_main(rank, world, port, q):
+    import torch.distributed as dist
+    sys.path.insert(0, str(ROOT))
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        q.put((rank, bench.max_over_ranks(1.5 + rank, dist, device="cpu")))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_two_gloo_ranks():
+    """bench.py's multi-GPU time is the slowest rank's: two gloo ranks on CPU."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    got = dict(q.get(timeout=10) for _ in range(2))
+    assert got == {0: 2.5, 1: 2.5}
+
+
+def test_max_over_ranks_single_process():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert bench.max_over_ranks(3.25, None) == 3.25
