@@ -250,6 +250,12 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
     std::vector<float> hy((size_t)ntraits * Np, 0.0f), hq((size_t)ntraits * Np, 0.0f);
     std::vector<uint32_t> hw((size_t)ntraits * Wp, 0u);
     ctx->qc.assign(ntraits, 0.0);
+    // Each centred trait is scaled by a power of two that brings its largest magnitude into
+    // [0.5, 1). F and F2 do not depend on the trait's scale, and a power-of-two factor is
+    // exact in binary floating point, so in the normal range every result is bit-identical
+    // to the unscaled computation; a trait in units of 1e20 or 1e-20 no longer overflows or
+    // underflows the single-precision sums of squares.
+    std::vector<double> p2s(ntraits, 1.0);
     for (int t = 0; t < ntraits; ++t) {
         const float *yt = y + (size_t)t * nid;
         const uint8_t *vt = valid ? valid + (size_t)t * nid : nullptr;
@@ -264,10 +270,15 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
             }
         }
         const double mu = nv ? sum / (double)nv : 0.0;
+        double maxabs = 0.0;
+        for (int k = 0; k < nid; ++k)
+            if (hw[(size_t)t * Wp + k / 32] >> (k % 32) & 1u) maxabs = std::max(maxabs, std::fabs((double)yt[k] - mu));
+        const double p2 = (maxabs > 0.0 && std::isfinite(maxabs)) ? std::ldexp(1.0, -(std::ilogb(maxabs) + 1)) : 1.0;
+        p2s[t] = p2;
         double s2 = 0.0;
         for (int k = 0; k < nid; ++k) {
             if (hw[(size_t)t * Wp + k / 32] >> (k % 32) & 1u) {
-                const float yc = (float)((double)yt[k] - mu);
+                const float yc = (float)(((double)yt[k] - mu) * p2);
                 hy[(size_t)t * Np + k] = yc;
                 s2 += (double)yc * (double)yc;
             }
@@ -300,9 +311,10 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
                 ++nv;
             }
         const double mu = nv ? sum / (double)nv : 0.0;
+        const double p2 = p2s[t];
         double maxabs = 0.0;
         for (int k = 0; k < nid; ++k)
-            if (ok(k)) maxabs = std::max(maxabs, std::fabs((double)yt[k] - mu));
+            if (ok(k)) maxabs = std::max(maxabs, std::fabs(((double)yt[k] - mu) * p2));
         const int sy = (maxabs > 0.0 && std::isfinite(maxabs)) ? (int)std::floor(std::log2(8355000.0 / maxabs)) : 0;
         const double scale = std::ldexp(1.0, sy);
         hsc[t] = std::ldexp(1.0, -sy);
@@ -310,7 +322,7 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
         double qmax = 0.0;
         for (int k = 0; k < nid; ++k) {
             if (!ok(k)) continue;
-            long long Y = std::llround(((double)yt[k] - mu) * scale);
+            long long Y = std::llround(((double)yt[k] - mu) * p2 * scale);
             Y = std::min(8355711LL, std::max(-8355711LL, Y));
             const long long a0 = ((Y + 128) & 255) - 128, Y1 = (Y - a0) / 256;
             const long long a1 = ((Y1 + 128) & 255) - 128, a2 = (Y1 - a1) / 256;

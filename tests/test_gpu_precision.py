@@ -98,3 +98,19 @@ def test_near_perfect_fit_is_a_hit(gpu_ctx, form, test):
     excl = parity.near_threshold(pb, blk, t1, t2, test, 1e-4)
     ok, msg = parity.compare_hit_lists(hits, hb, excl)
     assert ok, msg
+
+
+@pytest.mark.parametrize("form", [capi.FORM_POPC, capi.FORM_TENSOR], ids=["popc", "tensor"])
+@pytest.mark.parametrize("scale", [1e20, 1e-20], ids=["1e20", "1e-20"])
+def test_phenotype_scale(gpu_ctx, form, scale):
+    """F does not depend on the trait's units: a trait in units of 1e20 (squares beyond the
+    single-precision range) or 1e-20 (squares below it) gives the same hits and F as the FP64
+    oracle. The reference's float32 kernel overflows or underflows here, so only the FP64
+    oracle is compared."""
+    from test_gpu_parity import _check_block, _data
+    codes, gp, phen = _data(800, 60, seed=95)
+    scaled = np.where(phen == -9.0, np.float32(-9.0), phen * np.float32(scale)).astype(np.float32)
+    t1 = synth.f_threshold(8, 800 - 9, 1e-2)
+    t2 = synth.f_threshold(4, 800 - 9, 1e-2)
+    got = _check_block(gpu_ctx, codes, gp, scaled, (0, 60, 0, 60), "i", 0, t1, t2, form, check_ref=False)
+    assert len(got) > 0
