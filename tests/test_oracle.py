@@ -1,6 +1,7 @@
 """CPU tests of the oracles: oracle B (FP64 restatement) pinned against oracle A (the
-reference's own kernels built from its sources) and against the committed golden
-fixtures, plus the packing, file-format and permutation rules."""
+reference's own kernels built from its sources), plus the packing, file-format and
+permutation rules. The committed golden fixtures (reference outputs) are checked in
+test_golden.py."""
 import numpy as np
 import pytest
 
