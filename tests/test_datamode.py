@@ -128,3 +128,23 @@ def test_data_mode_errors(tmp_path):
     assert r.returncode != 0 and "not part of" in r.stdout
     r = run(CLI, "-Dr", ped, mp, ok=False)
     assert r.returncode != 0
+
+
+GOLDEN = ROOT / "tests" / "golden"
+PLINK_CASES = __import__("json").loads((GOLDEN / "plink_cases.json").read_text())
+
+
+@needs_cli
+@pytest.mark.parametrize("case", PLINK_CASES, ids=[c["name"] for c in PLINK_CASES])
+def test_read_plink_matches_golden(tmp_path, case):
+    """Against the reference's recorded outputs (tests/golden/, written by its own readplink.c
+    functions): no reference tree needed."""
+    import hashlib
+    ped, mp = write_plink(tmp_path, case["nid"], case["nsnp"], seed=case["seed"], **case["kw"])
+    assert hashlib.sha256(ped.read_bytes()).hexdigest() == case["ped_sha256"], "fileset generator changed"
+    assert hashlib.sha256(mp.read_bytes()).hexdigest() == case["map_sha256"], "fileset generator changed"
+    run(CLI, "-Dr", ped, mp, tmp_path / "ours.epigpu")
+    assert (tmp_path / "ours.epigpu").read_bytes() == (GOLDEN / ("%s.epigpu" % case["name"])).read_bytes()
+    run(CLI, "-De", tmp_path / "o.ped", tmp_path / "o.map", GOLDEN / ("%s.epigpu" % case["name"]))
+    assert (tmp_path / "o.ped").read_bytes() == (GOLDEN / ("%s.ped" % case["name"])).read_bytes()
+    assert (tmp_path / "o.map").read_bytes() == (GOLDEN / ("%s.map" % case["name"])).read_bytes()
