@@ -65,7 +65,9 @@ typedef struct epi_scan_opts {
     int32_t chunk;         /* -i iteration size (multiple of 16): only changes the output order */
     float t1;              /* -F threshold for F (8 df) */
     float t2;              /* -I threshold for F2 (4 df) */
-    int32_t form;          /* EPI_FORM_AUTO / _POPC (plain popcount form) / _TENSOR (tcgen05) */
+    int32_t form;          /* EPI_FORM_AUTO / _POPC (plain popcount form, up to 65,535 individuals)
+                            * / _TENSOR (tcgen05, up to 2^24 individuals); AUTO takes the tensor
+                            * form from 256 individuals on */
     int32_t report_trait;  /* trait whose hits are returned; -1 = every trait */
     int32_t reserved[9];   /* set to 0 */
 } epi_scan_opts;
