@@ -273,13 +273,17 @@ def run_reference(args):
     y = synth.phenotype(nid, seed=2, miss=0.01)
     t1, t2 = thresholds(nid)
     threads = os.cpu_count() or 1
-    # size the per-step sample to ~8 s on this host
-    probe = 150
-    t = time.perf_counter()
-    oracles.ref_scan_block(gp[:probe], nid, y, (0, probe, 0, probe), test=test, t1=t1, t2=t2, cap=1 << 16,
-                           nthreads=threads)
-    rate = probe * (probe - 1) / 2 / (time.perf_counter() - t)
-    m = int(min(nsnp, max(probe, (2 * rate * 8.0) ** 0.5)))
+    # size the per-step sample to ~8 s on this host; small probes run below the threads' full
+    # rate, so the size is refined from each probe until one takes at least half of that
+    m = 150
+    for _ in range(4):
+        t = time.perf_counter()
+        oracles.ref_scan_block(gp[:m], nid, y, (0, m, 0, m), test=test, t1=t1, t2=t2, cap=1 << 16,
+                               nthreads=threads)
+        dt = time.perf_counter() - t
+        if dt >= 4.0 or m >= nsnp:
+            break
+        m = int(min(nsnp, max(m + 1, (2 * (m * (m - 1) / 2) / dt * 8.0) ** 0.5)))
     pairs = m * (m - 1) // 2
     times = []
     for step in range(args.warmup + args.steps):
