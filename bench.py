@@ -428,7 +428,6 @@ def main():
             # (N=10,000, M=20,000, operands larger than L2) read and wrote 18.33 GB for
             # 199,990,000 pairs over Np = 10,112 padded individuals; the j rows are streamed
             # once per i tile, so the bytes scale with pairs x Np
-            # (profiles/scan_mma_traffic_cfg3m.md)
             np_pad = (nid + 127) // 128 * 128
             traffic = 18.33e9 / (199990000.0 * 10112.0) * pairs_launch * np_pad
             roof = {"bound": "tensor", "achieved": achieved, "peak": int8, "unit": "TOP/s",
