@@ -46,35 +46,13 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def gen_packed(nid, nsnp, seed, miss=0.01, chunk=4096):
-    """Seeded genotypes generated on the GPU (HWE, MAF ~ U(0.05, 0.5), `miss` missing calls),
-    packed in the reference layout into pinned host memory."""
-    import torch
-    dev = torch.device("cuda")
-    g = torch.Generator(device=dev)
-    g.manual_seed(seed)
-    npack, remain = divmod(nid, 16)
-    npack1 = npack + (1 if remain else 0)
-    out = torch.empty((nsnp, npack1), dtype=torch.int32, pin_memory=True)
-    shifts = torch.tensor([30 - 2 * t for t in range(16)], device=dev, dtype=torch.int64)
-    tsh = torch.tensor([2 * (remain - 1 - t) for t in range(remain)], device=dev, dtype=torch.int64)
-    for s0 in range(0, nsnp, chunk):
-        m = min(chunk, nsnp - s0)
-        f = torch.rand((m, 1), generator=g, device=dev) * 0.45 + 0.05
-        p0 = (1 - f) ** 2
-        p1 = p0 + 2 * f * (1 - f)
-        u = torch.rand((m, nid), generator=g, device=dev)
-        c = (u >= p0).to(torch.int64) + (u >= p1).to(torch.int64)
-        c[torch.rand((m, nid), generator=g, device=dev) < miss] = 3
-        parts = []
-        if npack:
-            parts.append((c[:, :16 * npack].reshape(m, npack, 16) << shifts).sum(-1))
-        if remain:
-            parts.append((c[:, 16 * npack:] << tsh).sum(-1, keepdim=True))
-        w = torch.cat(parts, 1)
-        w = torch.where(w >= 2 ** 31, w - 2 ** 32, w).to(torch.int32)
-        out[s0:s0 + m].copy_(w.cpu())
-    return out.numpy()
+# planted interacting pairs (snp1, snp2) and the share of the phenotypic variance each
+# explains: configuration 2 (5 pairs at 0.5%, two of them between the chromosomes) and
+# configuration 4 (3 pairs in column 0; the permuted columns carry none)
+PLANTED = {
+    "cfg2": ([(1500, 300), (12000, 4000), (18500, 11000), (10005, 9995), (9000, 8990)], 0.005),
+    "cfg4": ([(31000, 2000), (45000, 44000), (20000, 19000)], 0.02),
+}
 
 
 def workload_data(name, seed=1):
@@ -83,14 +61,22 @@ def workload_data(name, seed=1):
     if sizes is None:
         sizes = synth.uneven_block_sizes()
     nsnp = sum(sizes)
-    gp = gen_packed(nid, nsnp, seed=seed)
+    gp = synth.packed_on_gpu(nid, nsnp, seed=seed)
     rng = np.random.default_rng(seed + 7)
-    if ntraits == 1:
+    planted = PLANTED.get(name)
+    if ntraits == 1 and planted:
+        pairs, frac = planted
+        y = synth.planted_phenotype(synth.planted_rows(gp, nid, pairs), pairs, seed=seed + 1, var_frac=frac,
+                                    miss=0.01)
+        valid = None
+    elif ntraits == 1:
         y = synth.phenotype(nid, seed=seed + 1, miss=0.02 if name == "cfg1" else 0.01)
         valid = None
     elif name == "cfg4":
         from epigpu_b200 import capi
-        base = rng.standard_normal(nid).astype(np.float32)
+        pairs, frac = planted
+        base = synth.planted_phenotype(synth.planted_rows(gp, nid, pairs), pairs, seed=seed + 1, var_frac=frac,
+                                       miss=0.0)
         cols = [base] + [capi.permute_phenotype(base, p) for p in range(1, ntraits)]
         y = np.stack(cols, 1)
         valid = np.repeat((rng.random(nid) >= 0.01)[:, None], ntraits, 1)
@@ -108,7 +94,37 @@ def workload_data(name, seed=1):
     starts = np.cumsum([0] + sizes[:-1])
     blocks = [(int(starts[i]), sizes[i], int(starts[j]), sizes[j]) for i in range(len(sizes)) for j in range(i + 1)]
     return dict(nid=nid, nsnp=nsnp, sizes=sizes, test=test, ntraits=ntraits, desc=desc, gpack=gp, y=y,
-                valid=valid, blocks=blocks)
+                valid=valid, blocks=blocks, planted=planted[0] if planted else [])
+
+
+def f_error_sample(ctx, data, form, t1, t2, side=1000, seed=11):
+    """F and F2 of every pair of a seeded side x side block (side^2 pairs, both SNP ranges
+    inside the first chromosome block, the first above the second) from the GPU form against
+    the FP64 oracle, trait 0. Error per pair |F - F_oracle| / max(|F_oracle|, 1): relative
+    for F >= 1, absolute below; pairs with df1 = 0 (F undefined) are left out."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracles
+    from epigpu_b200 import capi, synth
+    nid, m0 = data["nid"], data["sizes"][0]
+    side = min(side, m0 // 2)
+    rng = np.random.default_rng(seed)
+    s2 = int(rng.integers(0, m0 // 2 - side + 1))
+    s1 = int(rng.integers(max(m0 // 2, s2 + side), m0 - side + 1))
+    blk = (s1, side, s2, side)
+    y = data["y"][:, 0] if data["y"].ndim == 2 else data["y"]
+    phen = y if data["valid"] is None else np.where(data["valid"][:, 0], y, np.float32(-9.0)).astype(np.float32)
+    d = ctx.scan_dump(blk, capi.default_opts(test="i", t1=t1, t2=t2, form=form), trait=0)
+    codes = synth.unpack(np.concatenate([data["gpack"][s2:s2 + side], data["gpack"][s1:s1 + side]]), nid)
+    _, _, pb = oracles.oracle_scan_block(codes, phen, (side, side, 0, side), test="i", t1=t1, t2=t2, per_pair=True)
+    out = {"pairs": side * side, "block": list(blk), "trait": 0,
+           "counts_exact": bool(np.array_equal(d["counts"], pb["counts"])),
+           "df_exact": bool(np.array_equal(d["df1"], pb["df1"]) and np.array_equal(d["df2"], pb["df2"]))}
+    ok = pb["df1"] > 0
+    for f in ("F", "F2"):
+        ref = pb[f][ok]
+        e = np.abs(d[f][ok].astype(np.float64) - ref) / np.maximum(np.abs(ref), 1.0)
+        out[f] = {"max": float(e.max()), "median": float(np.median(e))}
+    return out
 
 
 def thresholds(nid):
@@ -320,6 +336,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--popc-sample", type=int, default=20000,
                     help="SNPs in the square sample used to time the popcount form next to the tensor form")
+    ap.add_argument("--f-err-side", type=int, default=1000,
+                    help="side of the square block whose pairs' F error against the FP64 oracle is reported "
+                         "(0 = none)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -411,6 +430,10 @@ def main():
         ms, pp, _, _ = ctx.last_timing()
         popc = {"value": pp / (ms / 1e3), "unit": "pairs/s", "sample": "%d-SNP triangle" % m}
 
+    # planted pairs among the last step's hits (trait 0)
+    found = set(zip(hits["snp1"].tolist(), hits["snp2"].tolist()))
+    planted = {"pairs": len(data["planted"]), "recovered": sum(1 for p in data["planted"] if tuple(p) in found)}
+
     out = None
     if rank == 0:
         peaks, peak_kind = measured_peaks()
@@ -446,6 +469,9 @@ def main():
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(data, test, t1, t2)
+        ferr = None
+        if args.f_err_side > 0:
+            ferr = f_error_sample(ctx, data, form if form != capi.FORM_AUTO else used, t1, t2, side=args.f_err_side)
         out = {
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps, "higher_is_better": True,
@@ -455,7 +481,7 @@ def main():
                        "blocks": len(blocks), "traits": ntraits, "test": test, "t1": t1, "t2": t2,
                        "pairs_per_step": pairs_step, "form": used_form, "hits_per_step": int(nhits),
                        "l2": "inputs larger than L2 (packed genotypes %.0f MB)" % (gp.nbytes / 1e6),
-                       "gpu": gname},
+                       "gpu": gname, "planted": planted},
             "e2e": {"value": pairs_step * args.steps * world / e2e_s, "unit": "pairs/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
@@ -463,6 +489,7 @@ def main():
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clocks,
+            "f_err": ferr,
         }
         if popc:
             out["popc_form"] = popc

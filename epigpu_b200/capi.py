@@ -22,6 +22,7 @@ EPI_E_NODEVICE = 7
 EPI_E_UNSUPPORTED = 8
 
 FORM_AUTO, FORM_POPC, FORM_TENSOR = 0, 1, 2
+DEBUG_STALL = 1
 
 # Functions include/epigpu.h declares (checked by the CPU tests).
 EXPORTS = (
@@ -45,7 +46,8 @@ class Block(ctypes.Structure):
 class ScanOpts(ctypes.Structure):
     _fields_ = [("test", ctypes.c_int32), ("safe", ctypes.c_int32), ("chunk", ctypes.c_int32),
                 ("t1", ctypes.c_float), ("t2", ctypes.c_float), ("form", ctypes.c_int32),
-                ("report_trait", ctypes.c_int32), ("reserved", ctypes.c_int32 * 9)]
+                ("report_trait", ctypes.c_int32), ("wait_limit_ms", ctypes.c_int32), ("debug", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 7)]
 
 
 HIT_DTYPE = np.dtype([("snp1", "<i4"), ("snp2", "<i4"), ("df1", "<i4"), ("df2", "<i4"),
@@ -105,7 +107,8 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
 
 
-def default_opts(test="f", safe=0, chunk=128, t1=6.5, t2=10.5, form=FORM_AUTO, report_trait=0):
+def default_opts(test="f", safe=0, chunk=128, t1=6.5, t2=10.5, form=FORM_AUTO, report_trait=0, wait_limit_ms=0,
+                 debug=0):
     o = ScanOpts()
     load().epi_default_opts(ctypes.byref(o))
     o.test = ord(test) if isinstance(test, str) else int(test)
@@ -115,6 +118,8 @@ def default_opts(test="f", safe=0, chunk=128, t1=6.5, t2=10.5, form=FORM_AUTO, r
     o.t2 = float(t2)
     o.form = int(form)
     o.report_trait = int(report_trait)
+    o.wait_limit_ms = int(wait_limit_ms)
+    o.debug = int(debug)
     return o
 
 

@@ -434,6 +434,8 @@ epi_status check_opts(epi_ctx *ctx, const epi_scan_opts *o)
     if (o->form < EPI_FORM_AUTO || o->form > EPI_FORM_TENSOR) return set_err(ctx, EPI_E_INVALID, "bad form");
     if (o->report_trait < -1 || o->report_trait >= ctx->ntraits)
         return set_err(ctx, EPI_E_INVALID, "report_trait %d out of range", o->report_trait);
+    if (o->wait_limit_ms < 0) return set_err(ctx, EPI_E_INVALID, "wait_limit_ms must be >= 0");
+    if (o->debug != 0 && o->debug != EPI_DEBUG_STALL) return set_err(ctx, EPI_E_INVALID, "bad debug flags");
     return EPI_OK;
 }
 
@@ -527,6 +529,8 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     a.report_trait = o->report_trait;
     a.t1 = o->t1;
     a.t2 = o->t2;
+    a.wait_ns = o->wait_limit_ms > 0 ? (unsigned long long)o->wait_limit_ms * 1000000ull : 2000000000ull;
+    a.debug_stall = o->debug == EPI_DEBUG_STALL;
     a.counters = ctx->d_counters;
     a.maxf = ctx->d_maxf;
     a.maxf2 = ctx->d_maxf + ctx->ntraits;

@@ -82,6 +82,9 @@ struct ScanArgs {
     // test
     int32_t test_int, safe, report_trait;
     float t1, t2;
+    // tensor form: limit of every device-side wait (ns); test hook that makes one wait run out
+    unsigned long long wait_ns;
+    int32_t debug_stall;
     // outputs
     DevHit *hits;
     int64_t cap;

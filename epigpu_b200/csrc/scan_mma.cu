@@ -116,6 +116,7 @@ struct Smem {
     // the slot are done (both CTAs)
     uint64_t afull[ASTAGES], aempty[ASTAGES], bfull[BSTAGES], bempty[BSTAGES], raw_full[RSTAGES],
         raw_empty[RSTAGES], acc_full[2], acc_empty[2], drain;
+    uint64_t stall;  // never arrived at: the wait of the debug_stall test hook
     uint32_t tmem_base;
     int abort;
 };
@@ -356,6 +357,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             tc::mbar_init(&sm.acc_empty[b], 16);
         }
         tc::mbar_init(&sm.drain, 1);
+        tc::mbar_init(&sm.stall, 1);
         sm.abort = 0;
         tc::fence_barrier_init();
     }
@@ -375,7 +377,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             const Unit un = decode(a, u);
             if (un.skip) continue;
             for (int ks = 0; ks < nks; ++ks) {
-                if (!tc::mbar_wait(&sm.raw_full[rs], rph, abort) || !tc::mbar_wait(&sm.bempty[stage], phase ^ 1u, abort)) {
+                if (!tc::mbar_wait(&sm.raw_full[rs], rph, abort, a.wait_ns) || !tc::mbar_wait(&sm.bempty[stage], phase ^ 1u, abort, a.wait_ns)) {
                     fail(a, sm, 2);
                     ok = false;
                     break;
@@ -463,7 +465,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             const int gi = un.bd.start1 + (ivalid ? di : 0);
             // sum of (ytilde^2 - qcen) over the individuals known at SNP i
             const double pki = ivalid ? a.qtot[t] - a.qm[(size_t)t * a.nsnp + gi] : 0.0;
-            if (!tc::mbar_wait(&sm.acc_full[buf], accph[buf], abort)) {
+            if (!tc::mbar_wait(&sm.acc_full[buf], accph[buf], abort, a.wait_ns)) {
                 fail(a, sm, 3);
                 break;
             }
@@ -637,7 +639,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 if (un.skip) continue;
                 const int arow = 3 * (un.bd.start1 + un.i0 + TI * (int)rank);
                 for (int ks = 0; ks < nks; ++ks) {
-                    if (!tc::mbar_wait(&sm.aempty[as], aph ^ 1u, abort)) {
+                    if (!tc::mbar_wait(&sm.aempty[as], aph ^ 1u, abort, a.wait_ns)) {
                         fail(a, sm, 7);
                         ok = false;
                         break;
@@ -658,7 +660,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             int no_abort = 0;
             for (uint32_t back = 1; back <= ASTAGES && back <= issued_a; ++back) {
                 const uint32_t slot = (as + ASTAGES - back) % ASTAGES, par = back > as ? (aph ^ 1u) : aph;
-                if (!tc::mbar_wait(&sm.afull[slot], par, &no_abort)) fail(a, sm, 8);
+                if (!tc::mbar_wait(&sm.afull[slot], par, &no_abort, a.wait_ns)) fail(a, sm, 8);
             }
         }
     } else if (warp == 14) {
@@ -672,7 +674,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 const Unit un = decode(a, u);
                 if (un.skip) continue;
                 for (int ks = 0; ks < nks; ++ks) {
-                    if (!tc::mbar_wait(&sm.raw_empty[rs], rph ^ 1u, abort)) {
+                    if (!tc::mbar_wait(&sm.raw_empty[rs], rph ^ 1u, abort, a.wait_ns)) {
                         fail(a, sm, 10);
                         ok = false;
                         break;
@@ -688,7 +690,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             int no_abort = 0;
             for (uint32_t back = 1; back <= RSTAGES && back <= issued_r; ++back) {
                 const uint32_t slot = (rs + RSTAGES - back) % RSTAGES, par = back > rs ? (rph ^ 1u) : rph;
-                if (!tc::mbar_wait(&sm.raw_full[slot], par, &no_abort)) fail(a, sm, 11);
+                if (!tc::mbar_wait(&sm.raw_full[slot], par, &no_abort, a.wait_ns)) fail(a, sm, 11);
             }
         }
     } else if (lane == 0 && rank == 1) {
@@ -700,7 +702,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             const Unit un = decode(a, u);
             if (un.skip) continue;
             for (int ks = 0; ks < nks; ++ks) {
-                if (!tc::mbar_wait(&sm.afull[as], aph, abort)) {
+                if (!tc::mbar_wait(&sm.afull[as], aph, abort, a.wait_ns)) {
                     fail(a, sm, 9);
                     ok = false;
                     break;
@@ -714,18 +716,24 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         uint32_t as = 0, aph = 0, bs = 0, bph = 0, accph[2] = {0u, 0u};
         int buf = 0;
         bool ok = true;
+        // test hook: the first CTA pair's issuer waits on a barrier that nothing arrives at, so
+        // the wait runs out after wait_ns and the scan ends with a timeout status
+        if (a.debug_stall && pair == 0 && !tc::mbar_wait(&sm.stall, 0, abort, a.wait_ns)) {
+            fail(a, sm, 12);
+            ok = false;
+        }
         for (long long u = pair; u < units && ok; u += npairs) {
             const Unit un = decode(a, u);
             if (un.skip) continue;
-            if (!tc::mbar_wait_cluster(&sm.acc_empty[buf], accph[buf] ^ 1u, abort)) {
+            if (!tc::mbar_wait_cluster(&sm.acc_empty[buf], accph[buf] ^ 1u, abort, a.wait_ns)) {
                 fail(a, sm, 4);
                 break;
             }
             tc::tc_fence_after();
             const uint32_t d = tmem + acc_col(buf);
             for (int ks = 0; ks < nks; ++ks) {
-                if (!tc::mbar_wait_cluster(&sm.bfull[bs], bph, abort) ||
-                    !tc::mbar_wait_cluster(&sm.afull[as], aph, abort)) {
+                if (!tc::mbar_wait_cluster(&sm.bfull[bs], bph, abort, a.wait_ns) ||
+                    !tc::mbar_wait_cluster(&sm.afull[as], aph, abort, a.wait_ns)) {
                     fail(a, sm, 5);
                     ok = false;
                     break;
@@ -751,7 +759,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         // shared memory are released)
         tc::mma_commit_pair(&sm.drain);
         int no_abort = 0;
-        if (!tc::mbar_wait(&sm.drain, 0, &no_abort)) fail(a, sm, 6);
+        if (!tc::mbar_wait(&sm.drain, 0, &no_abort, a.wait_ns)) fail(a, sm, 6);
     }
 
     tc::tc_fence_before();

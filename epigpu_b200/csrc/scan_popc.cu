@@ -331,8 +331,23 @@ __device__ __forceinline__ void block_sum(double &v, long long &n, double *sv, l
     }
 }
 
+__device__ __forceinline__ double block_max(double v, double *sv)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sv[w] = v;
+    __syncthreads();
+    v = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) v = fmax(v, sv[i]);
+    return v;
+}
+
 // One block: resets the counters and maxima (every call starts from zero), writes the block
-// descriptor, then the centred phenotype as the library's epi_set_traits does on the host.
+// descriptor, then the centred phenotype as the library's epi_set_traits does on the host:
+// centred by the valid mean and scaled by the power of two that brings its largest magnitude
+// into [0.5, 1) (exact, so F and F2 are unchanged, and a trait in units of 1e20 or 1e-20
+// neither overflows nor underflows the single-precision squares).
 __global__ void __launch_bounds__(1024) k_prep(Scratch *s, const float *__restrict__ phen, int nid, int Np, int Wp,
                                                int safe, BlockDesc bd)
 {
@@ -353,12 +368,19 @@ __global__ void __launch_bounds__(1024) k_prep(Scratch *s, const float *__restri
     }
     block_sum(sum, n, sv, sn);
     const double mu = n ? sum / (double)n : 0.0;
+    double mx = 0.0;
+    for (int k = tid; k < nid; k += blockDim.x) {
+        const float y = phen[k];
+        if (safe || y != -9.0f) mx = fmax(mx, fabs((double)y - mu));
+    }
+    const double maxabs = block_max(mx, sv);
+    const double p2 = (maxabs > 0.0 && isfinite(maxabs)) ? ldexp(1.0, -(ilogb(maxabs) + 1)) : 1.0;
     double s2 = 0.0;
     long long dummy = 0;
     for (int k = tid; k < Np; k += blockDim.x) {
         const float y = k < nid ? phen[k] : -9.0f;
         const bool ok = k < nid && (safe || y != -9.0f);
-        const float yc = ok ? (float)((double)y - mu) : 0.0f;
+        const float yc = ok ? (float)(((double)y - mu) * p2) : 0.0f;
         s->y[k] = yc;
         if (ok) s2 += (double)yc * (double)yc;
     }
@@ -392,8 +414,7 @@ __global__ void k_finish(const Scratch *s, int64_t *nhits, float *maxf, int test
 }
 
 constexpr int MAX_DEVICES = 64;
-static Scratch *g_addr[MAX_DEVICES];  // device address of g_scratch, per device (set-up)
-static int g_sms[MAX_DEVICES];
+static int g_sms[MAX_DEVICES];  // per device: SM count, 0 until the device's set-up ran
 
 }  // namespace noalloc
 }  // namespace epi
@@ -410,26 +431,33 @@ extern "C" epi_status epi_scan_block_noalloc(const int32_t *d_gpack, int32_t nid
     if (block->start1 < 0 || block->start2 < 0 || block->size1 < 0 || block->size2 < 0 ||
         (int64_t)block->start1 + block->size1 > nsnp || (int64_t)block->start2 + block->size2 > nsnp)
         return EPI_E_INVALID;
+    // an error left pending by the caller's earlier work is theirs: report it, do not clear it
+    if (cudaPeekAtLastError() != cudaSuccess) return EPI_E_CUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= noalloc::MAX_DEVICES) return EPI_E_NODEVICE;
     cudaStream_t st = (cudaStream_t)stream;
     const size_t smem = sizeof(popc::Smem) + 8;  // + per-CTA maxima of one trait
 
-    // once per device, with that device current: the scratch's device address
-    if (noalloc::g_addr[dev] == nullptr) {
+    // set-up, once per device with that device current: the device check, the SM count and
+    // the kernel's shared-memory attribute
+    if (noalloc::g_sms[dev] == 0) {
         int major = 0, sms = 0;
         if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess || major != 10)
             return EPI_E_NODEVICE;
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return EPI_E_CUDA;
-        void *ptr = nullptr;
-        if (cudaGetSymbolAddress(&ptr, noalloc::g_scratch) != cudaSuccess || ptr == nullptr) return EPI_E_CUDA;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+            return EPI_E_CUDA;
         if (cudaFuncSetAttribute(popc::k_scan_popc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
             cudaSuccess)
             return EPI_E_CUDA;
         noalloc::g_sms[dev] = sms;
-        noalloc::g_addr[dev] = (noalloc::Scratch *)ptr;
     }
-    noalloc::Scratch *scr = noalloc::g_addr[dev];
+    // The scratch array's device address. In host code g_scratch only stands for the array;
+    // the address comes from the runtime, for the current device. It is looked up on every
+    // call (a host-side table lookup once the module is loaded), so that a device reset
+    // between calls, which reloads the module, cannot leave a stale address behind.
+    void *ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, noalloc::g_scratch) != cudaSuccess || ptr == nullptr) return EPI_E_CUDA;
+    noalloc::Scratch *scr = (noalloc::Scratch *)ptr;
 
     const int Wp = ((nid + 31) / 32 + 3) / 4 * 4;
     const int Np = 32 * Wp;
@@ -478,9 +506,11 @@ extern "C" epi_status epi_scan_block_noalloc(const int32_t *d_gpack, int32_t nid
     }
     noalloc::k_finish<<<1, 32, 0, st>>>(scr, d_nhits, d_maxf, a.test_int);
     if (cudaGetLastError() != cudaSuccess) return EPI_E_CUDA;
-    unsigned long long flags[2] = {0ull, 0ull};
-    if (cudaMemcpyAsync(flags, &scr->counters[2], sizeof(flags), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    unsigned long long found = 0ull;
+    if (cudaMemcpyAsync(&found, &scr->counters[0], sizeof(found), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return EPI_E_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return EPI_E_CUDA;
-    return flags[0] ? EPI_E_TIMEOUT : EPI_OK;
+    // as epi_scan: more hits than `cap` is reported (the first `cap` rows are written, and
+    // *d_nhits holds the total)
+    return (int64_t)found > cap ? EPI_E_OVERFLOW : EPI_OK;
 }

@@ -1,14 +1,15 @@
 // tc_ptx.cuh -- thin inline-PTX wrappers for the sm_100a features the tensor-core scan
 // uses: mbarriers, clusters, tcgen05 (pair TMEM alloc, ld, MMA, commit, fences) and proxy fences.
-// Every wait is bounded: it gives up after `kWaitNs` nanoseconds of %globaltimer and
-// reports failure to the caller, which records an error and leaves its loop.
+// Every wait is bounded: it gives up after `limit_ns` nanoseconds of %globaltimer (a kernel
+// argument, kDefaultWaitNs unless the caller asks for less) and reports failure to the
+// caller, which records an error and leaves its loop.
 #pragma once
 #include <cstdint>
 
 namespace epi {
 namespace tc {
 
-constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s: legitimate waits last microseconds
+constexpr unsigned long long kDefaultWaitNs = 2000000000ull;  // 2 s: legitimate waits last microseconds
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -46,16 +47,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Waits for the phase of `bar` with parity `parity` to complete. Returns false on timeout
-// or when *abort becomes non-zero (another role gave up).
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort)
+// Waits for the phase of `bar` with parity `parity` to complete. Returns false after
+// `limit_ns` or when *abort becomes non-zero (another role gave up).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort,
+                                          unsigned long long limit_ns)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer();
     for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
         if (*abort) return false;
-        if (globaltimer() - t0 > kWaitNs) return false;
+        if (globaltimer() - t0 > limit_ns) return false;
     }
 }
 
@@ -145,14 +147,15 @@ __device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t *bar, uint32_t pa
 }
 
 // mbar_wait for a barrier that also receives arrivals from the other CTA of the cluster
-__device__ __forceinline__ bool mbar_wait_cluster(uint64_t *bar, uint32_t parity, volatile int *abort)
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t *bar, uint32_t parity, volatile int *abort,
+                                                  unsigned long long limit_ns)
 {
     if (mbar_try_wait_cluster(bar, parity)) return true;
     const unsigned long long t0 = globaltimer();
     for (;;) {
         if (mbar_try_wait_cluster(bar, parity)) return true;
         if (*abort) return false;
-        if (globaltimer() - t0 > kWaitNs) return false;
+        if (globaltimer() - t0 > limit_ns) return false;
     }
 }
 

@@ -21,9 +21,6 @@ int UDEVICE = 0;
 int UCHUNKSIZE = 128;
 int UTEST = 'f';
 int USAFE = 0;
-int UFORM = EPI_FORM_AUTO;
-int UNPERM = 0;
-int UREFRESUME = 0;
 char plinkbin[100];
 float UTHRESHOLD1 = 6.5f, UTHRESHOLD2 = 10.5f;
 char UPHEN[1000];

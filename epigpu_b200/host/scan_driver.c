@@ -32,6 +32,14 @@
 
 #define PAIR_BATCH ((long long)1 << 34) /* pairs per launch batch between checkpoints */
 
+/* Settings this build adds to the reference's globals (src/epiopencl.h:9-16, which the
+ * caller's main.c defines). They are defined here, with their defaults, so that the
+ * reference's own main.c links against this file unchanged: the GPU form (-g), the
+ * permutation-threshold count (-N) and the reference's resume rule (-R). */
+int UFORM = EPI_FORM_AUTO;
+int UNPERM = 0;
+int UREFRESUME = 0;
+
 static void fail(epi_ctx *ctx, epi_status st, const char *what)
 {
     if (st == EPI_E_NODEVICE) {

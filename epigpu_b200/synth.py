@@ -80,9 +80,10 @@ def phenotype(nid, seed, miss=0.02, dist="normal"):
 
 def planted_phenotype(codes, pairs, seed, var_frac=0.005, miss=0.01):
     """N(0,1) noise plus one random mean-0 3x3 genotype-class effect per planted pair
-    (snp_a, snp_b), each scaled to explain `var_frac` of the phenotypic variance."""
+    (snp_a, snp_b), each scaled to explain `var_frac` of the phenotypic variance.
+    `codes[s]` is SNP s's row of codes: the (nsnp, nid) array or a dict of the planted rows."""
     rng = np.random.default_rng(seed)
-    nid = codes.shape[1]
+    nid = len(codes[pairs[0][0]])
     y = rng.standard_normal(nid)
     for a, b in pairs:
         ga, gb = codes[a].astype(np.int64), codes[b].astype(np.int64)
@@ -112,3 +113,43 @@ def uneven_block_sizes():
     sizes = [int(round(2000 + 22000 * ((21 - c) / 21.0) ** 1.3705)) for c in range(22)]
     sizes[0] += 250000 - sum(sizes)
     return sizes
+
+
+def planted_rows(gpack, nid, pairs):
+    """The code rows of the planted SNPs, unpacked from packed genotypes (a dict for
+    planted_phenotype when the whole code matrix is not kept)."""
+    snps = sorted({s for p in pairs for s in p})
+    rows = unpack(np.asarray(gpack)[snps], nid)
+    return {s: rows[i] for i, s in enumerate(snps)}
+
+
+def packed_on_gpu(nid, nsnp, seed, miss=0.01, chunk=4096):
+    """The genotype generator above (HWE, MAF ~ U(0.05, 0.5), `miss` missing calls) drawn on
+    the GPU with torch's generator, packed in the reference layout into pinned host memory:
+    the inputs of full-size runs, which numpy would take minutes to draw."""
+    import torch
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    npack, remain = divmod(nid, 16)
+    npack1 = npack + (1 if remain else 0)
+    out = torch.empty((nsnp, npack1), dtype=torch.int32, pin_memory=True)
+    shifts = torch.tensor([30 - 2 * t for t in range(16)], device=dev, dtype=torch.int64)
+    tsh = torch.tensor([2 * (remain - 1 - t) for t in range(remain)], device=dev, dtype=torch.int64)
+    for s0 in range(0, nsnp, chunk):
+        m = min(chunk, nsnp - s0)
+        f = torch.rand((m, 1), generator=g, device=dev) * 0.45 + 0.05
+        p0 = (1 - f) ** 2
+        p1 = p0 + 2 * f * (1 - f)
+        u = torch.rand((m, nid), generator=g, device=dev)
+        c = (u >= p0).to(torch.int64) + (u >= p1).to(torch.int64)
+        c[torch.rand((m, nid), generator=g, device=dev) < miss] = 3
+        parts = []
+        if npack:
+            parts.append((c[:, :16 * npack].reshape(m, npack, 16) << shifts).sum(-1))
+        if remain:
+            parts.append((c[:, 16 * npack:] << tsh).sum(-1, keepdim=True))
+        w = torch.cat(parts, 1)
+        w = torch.where(w >= 2 ** 31, w - 2 ** 32, w).to(torch.int32)
+        out[s0:s0 + m].copy_(w.cpu())
+    return out.numpy()

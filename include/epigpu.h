@@ -69,8 +69,15 @@ typedef struct epi_scan_opts {
                             * / _TENSOR (tcgen05, up to 2^24 individuals); AUTO takes the tensor
                             * form from 256 individuals on */
     int32_t report_trait;  /* trait whose hits are returned; -1 = every trait */
-    int32_t reserved[9];   /* set to 0 */
+    int32_t wait_limit_ms; /* tensor form: every device-side wait gives up after this many
+                            * milliseconds and the scan returns EPI_E_TIMEOUT; 0 = 2000 */
+    int32_t debug;         /* 0; EPI_DEBUG_STALL (tests of the timeout path only): one wait of
+                            * the tensor form is on a barrier nothing arrives at, so it runs
+                            * out after wait_limit_ms and the scan returns EPI_E_TIMEOUT */
+    int32_t reserved[7];   /* set to 0 */
 } epi_scan_opts;
+
+#define EPI_DEBUG_STALL 1
 
 /* Fills `o` with the reference defaults: 'f', normal mode, chunk 128, F 6.5, I 10.5
  * (src/main.c:244-249), AUTO form, trait 0. */
@@ -166,16 +173,20 @@ epi_status epi_get_stream(const epi_ctx *ctx, void **stream);
  *   opts     test, safe, t1, t2 as for epi_scan (form and chunk are ignored)
  *   d_hits   device, cap rows: the hits, in no particular order (epi_scan gives the
  *            reference's order; sort by (snp1, snp2) to compare)
- *   d_nhits  device, one int64: the number of hits (may exceed cap; rows past cap are
- *            dropped)
+ *   d_nhits  device, one int64: the number of hits; when it exceeds cap the first cap
+ *            rows are written and the call returns EPI_E_OVERFLOW, as epi_scan does
  *   d_maxf   device, nullable, 2 floats: largest F and F2 over the block
  *
  * Working memory is a fixed array of about 520 KiB in this library, one per device, held
  * until the process exits: it limits nid to EPI_NOALLOC_MAX_NID (larger returns
- * EPI_E_UNSUPPORTED). The first call on each device looks up that array's device address;
- * make that first call before any CUDA stream capture. All calls on a device share the
- * array: calls that overlap on the GPU (other host threads, other streams) race and must
- * be serialised by the caller.
+ * EPI_E_UNSUPPORTED). The first call on each device does that device's set-up (device
+ * check, SM count, kernel attribute); make that first call before any CUDA stream capture.
+ * Every call looks up the array's device address for the current device. All calls on a
+ * device share the array and each call clears what it needs, so results never carry over,
+ * but calls that overlap on the GPU (other host threads, other streams) race and must be
+ * serialised by the caller. The call waits for the scan to finish (it synchronises
+ * `stream`) before it returns. A CUDA error already pending from the caller's earlier work
+ * makes it return EPI_E_CUDA at once, leaving that error pending.
  */
 #define EPI_NOALLOC_MAX_NID 65535
 epi_status epi_scan_block_noalloc(const int32_t *d_gpack, int32_t nid, int32_t nsnp,

@@ -1,6 +1,7 @@
 """Build oracle A from the reference's own sources -- TEST INFRASTRUCTURE.
 
-Reads src/EpiOpenCL.c of the reference (read-only, default /root/reference), decodes
+Reads src/EpiOpenCL.c of the reference tree (read-only; --reference or the EPIGPU_REFERENCE
+environment variable), decodes
 the C string literals that hold the OpenCL pair kernels
 
     kernelfull      src/EpiOpenCL.c:45-264   (8 df)
@@ -13,7 +14,7 @@ and compiles each one unmodified as C99 behind ref_prelude.h, renaming its entry
 oracle/_ref/libepiref.so. The decoded kernel text only lives in a temporary directory;
 the only output is the shared library under oracle/_ref/ (git-ignored, never committed).
 
-Usage: python oracle/build_ref.py [--reference DIR]
+Usage: python oracle/build_ref.py --reference DIR   (or EPIGPU_REFERENCE=DIR)
 """
 import argparse
 import os
@@ -104,8 +105,10 @@ def build(reference: pathlib.Path, out_dir: pathlib.Path = OUT_DIR, quiet: bool 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("EPIGPU_REFERENCE"))
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give the reference tree: --reference DIR or EPIGPU_REFERENCE=DIR")
     ref = pathlib.Path(args.reference)
     if not (ref / "src" / "EpiOpenCL.c").exists():
         print("reference sources not found at", ref, file=sys.stderr)

@@ -154,22 +154,38 @@ int64_t oracle_scan_block(int test, int safe, int chunk, const uint8_t *geno, in
                           int32_t *out_df1, int32_t *out_df2)
 {
     const int L = safe ? 8 : 16;
-    int64_t nh = 0, capk = 1024;
-    okey_hit *kh = (okey_hit *)malloc(sizeof(okey_hit) * (size_t)capk);
+    const size_t np = (size_t)chr1m * (size_t)chr2m;
+    /* pass 1, rows in parallel: every pair's statistics (into the caller's arrays, or
+     * scratch ones); pass 2, serial: the hit rule and the output order */
+    double *pF = out_F ? out_F : (double *)malloc(sizeof(double) * (np ? np : 1));
+    double *pF2 = out_F2 ? out_F2 : (double *)malloc(sizeof(double) * (np ? np : 1));
+    int32_t *pd1 = out_df1 ? out_df1 : (int32_t *)malloc(sizeof(int32_t) * (np ? np : 1));
+    int32_t *pd2 = out_df2 ? out_df2 : (int32_t *)malloc(sizeof(int32_t) * (np ? np : 1));
+#pragma omp parallel for schedule(dynamic, 1)
     for (int gx = 0; gx < chr1m; gx++) {
         for (int gy = 0; gy < chr2m; gy++) {
             if (!(gx + chr1g > gy + chr2g)) continue;
             int32_t cnt[9];
             double F, F2;
             int d1, d2;
-            int nfac = oracle_pair(geno + (size_t)(gx + chr1g) * nid, geno + (size_t)(gy + chr2g) * nid,
-                                   phen, nid, safe, cnt, NULL, &F, &F2, &d1, &d2);
+            oracle_pair(geno + (size_t)(gx + chr1g) * nid, geno + (size_t)(gy + chr2g) * nid, phen, nid, safe, cnt,
+                        NULL, &F, &F2, &d1, &d2);
             size_t o = (size_t)gx * chr2m + gy;
             if (out_counts) memcpy(out_counts + 9 * o, cnt, sizeof(cnt));
-            if (out_F) out_F[o] = F;
-            if (out_F2) out_F2[o] = F2;
-            if (out_df1) out_df1[o] = d1;
-            if (out_df2) out_df2[o] = d2;
+            pF[o] = F;
+            pF2[o] = F2;
+            pd1[o] = d1;
+            pd2[o] = d2;
+        }
+    }
+    int64_t nh = 0, capk = 1024;
+    okey_hit *kh = (okey_hit *)malloc(sizeof(okey_hit) * (size_t)capk);
+    for (int gx = 0; gx < chr1m; gx++) {
+        for (int gy = 0; gy < chr2m; gy++) {
+            if (!(gx + chr1g > gy + chr2g)) continue;
+            size_t o = (size_t)gx * chr2m + gy;
+            const double F = pF[o], F2 = pF2[o];
+            const int d1 = pd1[o], d2 = pd2[o], nfac = d1 + 1;
             int hit;
             if (test == 'f') hit = F > (double)t1;
             else hit = (F > (double)t1 || F2 > (double)t2) && (safe || nfac > 6);
@@ -195,6 +211,10 @@ int64_t oracle_scan_block(int test, int safe, int chunk, const uint8_t *geno, in
     qsort(kh, (size_t)nh, sizeof(okey_hit), okey_cmp);
     for (int64_t i = 0; i < nh && i < cap; i++) hits[i] = kh[i].h;
     free(kh);
+    if (!out_F) free(pF);
+    if (!out_F2) free(pF2);
+    if (!out_df1) free(pd1);
+    if (!out_df2) free(pd2);
     return nh;
 }
 
