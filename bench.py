@@ -334,6 +334,8 @@ def main():
     ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
     ap.add_argument("--form", default="auto", choices=["auto", "popc", "tensor"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch each scan's device work directly instead of replaying its captured CUDA graph")
     ap.add_argument("--popc-sample", type=int, default=20000,
                     help="SNPs in the square sample used to time the popcount form next to the tensor form")
     ap.add_argument("--f-err-side", type=int, default=1000,
@@ -362,7 +364,7 @@ def main():
     gname, sms = ctx.device_info()
     gp, y, valid = data["gpack"], data["y"], data["valid"]
     ntraits = data["ntraits"]
-    opts = capi.default_opts(test=test, t1=t1, t2=t2, form=form, report_trait=0)
+    opts = capi.default_opts(test=test, t1=t1, t2=t2, form=form, report_trait=0, no_graph=int(args.no_graph))
     blocks = data["blocks"]
     pairs_step = sum(block_pairs(b) for b in blocks) * ntraits
 
@@ -481,7 +483,7 @@ def main():
                        "blocks": len(blocks), "traits": ntraits, "test": test, "t1": t1, "t2": t2,
                        "pairs_per_step": pairs_step, "form": used_form, "hits_per_step": int(nhits),
                        "l2": "inputs larger than L2 (packed genotypes %.0f MB)" % (gp.nbytes / 1e6),
-                       "gpu": gname, "planted": planted},
+                       "gpu": gname, "planted": planted, "cuda_graph": not args.no_graph},
             "e2e": {"value": pairs_step * args.steps * world / e2e_s, "unit": "pairs/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),

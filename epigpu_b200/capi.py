@@ -47,7 +47,7 @@ class ScanOpts(ctypes.Structure):
     _fields_ = [("test", ctypes.c_int32), ("safe", ctypes.c_int32), ("chunk", ctypes.c_int32),
                 ("t1", ctypes.c_float), ("t2", ctypes.c_float), ("form", ctypes.c_int32),
                 ("report_trait", ctypes.c_int32), ("wait_limit_ms", ctypes.c_int32), ("debug", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 7)]
+                ("no_graph", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
 
 
 HIT_DTYPE = np.dtype([("snp1", "<i4"), ("snp2", "<i4"), ("df1", "<i4"), ("df2", "<i4"),
@@ -108,7 +108,7 @@ def _ptr(a):
 
 
 def default_opts(test="f", safe=0, chunk=128, t1=6.5, t2=10.5, form=FORM_AUTO, report_trait=0, wait_limit_ms=0,
-                 debug=0):
+                 debug=0, no_graph=0):
     o = ScanOpts()
     load().epi_default_opts(ctypes.byref(o))
     o.test = ord(test) if isinstance(test, str) else int(test)
@@ -120,6 +120,7 @@ def default_opts(test="f", safe=0, chunk=128, t1=6.5, t2=10.5, form=FORM_AUTO, r
     o.report_trait = int(report_trait)
     o.wait_limit_ms = int(wait_limit_ms)
     o.debug = int(debug)
+    o.no_graph = int(no_graph)
     return o
 
 

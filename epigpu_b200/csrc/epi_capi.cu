@@ -24,7 +24,13 @@ cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int 
                           cudaStream_t stream);
 cudaError_t launch_qmiss(const uint32_t *missbits, int nsnp, int Wp, const uint32_t *wmask, const double *qd,
                         const double *qr, int Np, int ntraits, double *qm, double *rm, cudaStream_t stream);
-cudaError_t launch_popc(const ScanArgs &a, int grid, cudaStream_t stream);
+cudaError_t launch_major(const uint4 *planes, int nsnp, int Wp, uint8_t *maj, cudaStream_t stream);
+cudaError_t launch_marg(const uint4 *planes, int nsnp, int Wp, const float *y, const uint32_t *wmask, int Np,
+                        int ntraits, double *pmC, int32_t *pmN, double *pmQ, cudaStream_t stream);
+// plain form (scan_popc.cu)
+cudaError_t popc_prepare();
+cudaError_t popc_enqueue(const ScanArgs &a, const PopcMaps &maps, int grid, cudaStream_t stream);
+cudaError_t popc_encode_planes(PopcMaps *maps, const uint4 *planes, int nsnp, int Wp);
 int popc_tile_i();
 int popc_tile_j();
 // tensor form (scan_mma.cu)
@@ -33,9 +39,17 @@ int mma_tile_i();
 int mma_tile_j();
 int mma_min_nid();
 int mma_max_nid();
-cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream);
+cudaError_t mma_prepare(int ntraits, int grid_request, int *grid);
+cudaError_t mma_enqueue(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream);
 cudaError_t mma_encode_genotypes(MmaMaps *maps, const uint8_t *hcodes, const uint8_t *h3, int nsnp, int Np);
 cudaError_t mma_encode_traits(MmaMaps *maps, const int8_t *ydig, int ntraits, int Np);
+// Start of a scan: counters (hits, tile queue, error flag and site) to zero, the per-trait
+// maxima of F and F2 to the order-encoded -inf.
+__global__ void k_scan_init(unsigned long long *counters, unsigned int *maxf, int n)
+{
+    if (threadIdx.x < 4) counters[threadIdx.x] = 0ull;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) maxf[i] = 0x007fffffu;
+}
 }  // namespace epi
 
 using epi::BlockDesc;
@@ -55,7 +69,9 @@ struct epi_ctx {
     uint4 *d_planes = nullptr;
     uint8_t *d_hcodes = nullptr, *d_h3 = nullptr;
     uint32_t *d_missbits = nullptr;
-    size_t planes_cap = 0, hcodes_cap = 0, h3_cap = 0, missbits_cap = 0;
+    uint8_t *d_maj = nullptr;
+    size_t planes_cap = 0, hcodes_cap = 0, h3_cap = 0, missbits_cap = 0, maj_cap = 0;
+    epi::PopcMaps pmaps;
     // traits
     int ntraits = 0, traits_nid = 0;
     float *d_y = nullptr, *d_q = nullptr;
@@ -67,6 +83,11 @@ struct epi_ctx {
     bool qm_valid = false;
     epi::MmaMaps maps;
     std::vector<double> qc;
+    // plain form: marginals per (trait, SNP) and the sum of y^2 per trait
+    double *d_pmC = nullptr, *d_pmQ = nullptr, *d_ysq = nullptr;
+    int32_t *d_pmN = nullptr;
+    size_t pmC_cap = 0, pmQ_cap = 0, pmN_cap = 0, ysq_cap = 0;
+    bool pm_valid = false;
     // scan scratch
     DevHit *d_hits = nullptr;
     int64_t hit_cap = 0;
@@ -75,6 +96,15 @@ struct epi_ctx {
     int maxf_cap = 0;
     BlockDesc *d_blocks = nullptr;
     int blocks_cap = 0;
+    // pinned host staging of the device part of a scan: the block schedule it uploads, the
+    // counters and maxima it reads back
+    BlockDesc *h_blocks = nullptr;
+    int h_blocks_cap = 0;
+    unsigned long long *h_state = nullptr;  // counters[4], then 2 x ntraits encoded maxima
+    size_t h_state_cap = 0;
+    // the device part of the last scan, captured as a CUDA graph, and what it was captured for
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<unsigned char> gkey;
     // last scan
     double last_ms = 0.0;
     int64_t last_pairs = 0;
@@ -185,9 +215,13 @@ epi_status epi_close(epi_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     void *bufs[] = {ctx->d_raw, ctx->d_planes, ctx->d_hcodes, ctx->d_h3, ctx->d_missbits, ctx->d_y, ctx->d_q,
                     ctx->d_wmask, ctx->d_qc, ctx->d_yscale, ctx->d_qd, ctx->d_qtot, ctx->d_qm, ctx->d_ydig,
-                    ctx->d_hits, ctx->d_counters, ctx->d_maxf, ctx->d_blocks};
+                    ctx->d_hits, ctx->d_counters, ctx->d_maxf, ctx->d_blocks, ctx->d_maj, ctx->d_pmC,
+                    ctx->d_pmQ, ctx->d_ysq, ctx->d_pmN};
     for (void *p : bufs)
         if (p) cudaFree(p);
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    if (ctx->h_blocks) cudaFreeHost(ctx->h_blocks);
+    if (ctx->h_state) cudaFreeHost(ctx->h_state);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -221,12 +255,16 @@ epi_status epi_load_packed(epi_ctx *ctx, const int32_t *gpack, int32_t nid, int3
     CK(ensure(&ctx->d_hcodes, &ctx->hcodes_cap, (size_t)nsnp * Wp * 32));
     CK(ensure(&ctx->d_h3, &ctx->h3_cap, 3 * (size_t)nsnp * Wp * 32));
     CK(ensure(&ctx->d_missbits, &ctx->missbits_cap, (size_t)nsnp * Wp * sizeof(uint32_t)));
+    CK(ensure(&ctx->d_maj, &ctx->maj_cap, (size_t)nsnp));
     CK(cudaMemcpyAsync(ctx->d_raw, gpack, (size_t)nsnp * npack1 * sizeof(int32_t), cudaMemcpyHostToDevice,
                        ctx->stream));
     CK(epi::launch_unpack(ctx->d_raw, nsnp, nid, npack, remain, ctx->d_planes, Wp, nullptr, Wc, ctx->d_hcodes,
                           ctx->d_h3, ctx->d_missbits, ctx->stream));
+    CK(epi::launch_major(ctx->d_planes, nsnp, Wp, ctx->d_maj, ctx->stream));
     ctx->qm_valid = false;
+    ctx->pm_valid = false;
     CK(epi::mma_encode_genotypes(&ctx->maps, ctx->d_hcodes, ctx->d_h3, nsnp, 32 * Wp));
+    CK(epi::popc_encode_planes(&ctx->pmaps, ctx->d_planes, nsnp, Wp));
     if (ctx->traits_nid != nid) ctx->ntraits = 0;  // traits no longer match
     ctx->nid = nid;
     ctx->nsnp = nsnp;
@@ -255,7 +293,7 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
     // exact in binary floating point, so in the normal range every result is bit-identical
     // to the unscaled computation; a trait in units of 1e20 or 1e-20 no longer overflows or
     // underflows the single-precision sums of squares.
-    std::vector<double> p2s(ntraits, 1.0);
+    std::vector<double> p2s(ntraits, 1.0), ysq(ntraits, 0.0);
     for (int t = 0; t < ntraits; ++t) {
         const float *yt = y + (size_t)t * nid;
         const uint8_t *vt = valid ? valid + (size_t)t * nid : nullptr;
@@ -285,6 +323,7 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
         }
         const double c = nv ? s2 / (double)nv : 0.0;
         ctx->qc[t] = c;
+        ysq[t] = s2;
         for (int k = 0; k < nid; ++k) {
             if (hw[(size_t)t * Wp + k / 32] >> (k % 32) & 1u) {
                 const double yc = hy[(size_t)t * Np + k];
@@ -365,6 +404,8 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
     CK(cudaMemcpyAsync(ctx->d_q, hq.data(), need, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->d_wmask, hw.data(), hw.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->d_qc, ctx->qc.data(), ntraits * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(ensure(&ctx->d_ysq, &ctx->ysq_cap, (size_t)ntraits * sizeof(double)));
+    CK(cudaMemcpyAsync(ctx->d_ysq, ysq.data(), ntraits * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(ensure(&ctx->d_ydig, &ctx->ydig_cap, hd.size()));
     CK(ensure(&ctx->d_qd, &ctx->qd_cap, hqd.size() * sizeof(double)));
     CK(ensure(&ctx->d_qtot, &ctx->qtot_cap, (size_t)ntraits * sizeof(double)));
@@ -378,6 +419,7 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
     ctx->ntraits = ntraits;
     ctx->traits_nid = nid;
     ctx->qm_valid = false;
+    ctx->pm_valid = false;
     return EPI_OK;
 }
 
@@ -436,6 +478,7 @@ epi_status check_opts(epi_ctx *ctx, const epi_scan_opts *o)
         return set_err(ctx, EPI_E_INVALID, "report_trait %d out of range", o->report_trait);
     if (o->wait_limit_ms < 0) return set_err(ctx, EPI_E_INVALID, "wait_limit_ms must be >= 0");
     if (o->debug != 0 && o->debug != EPI_DEBUG_STALL) return set_err(ctx, EPI_E_INVALID, "bad debug flags");
+    if (o->no_graph != 0 && o->no_graph != 1) return set_err(ctx, EPI_E_INVALID, "no_graph must be 0 or 1");
     return EPI_OK;
 }
 
@@ -481,9 +524,21 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     size_t bcap = (size_t)ctx->blocks_cap * sizeof(BlockDesc);
     CK(ensure(&ctx->d_blocks, &bcap, (size_t)std::max(nblocks, 1) * sizeof(BlockDesc)));
     ctx->blocks_cap = (int)(bcap / sizeof(BlockDesc));
-    if (nblocks)
-        CK(cudaMemcpyAsync(ctx->d_blocks, r.desc.data(), nblocks * sizeof(BlockDesc), cudaMemcpyHostToDevice,
-                           ctx->stream));
+    if (ctx->h_blocks_cap < nblocks) {
+        if (ctx->h_blocks) cudaFreeHost(ctx->h_blocks);
+        ctx->h_blocks = nullptr;
+        ctx->h_blocks_cap = 0;
+        CK(cudaHostAlloc((void **)&ctx->h_blocks, (size_t)nblocks * sizeof(BlockDesc), cudaHostAllocDefault));
+        ctx->h_blocks_cap = nblocks;
+    }
+    const size_t state = 4 * sizeof(unsigned long long) + 2 * (size_t)ctx->ntraits * sizeof(unsigned int);
+    if (ctx->h_state_cap < state) {
+        if (ctx->h_state) cudaFreeHost(ctx->h_state);
+        ctx->h_state = nullptr;
+        ctx->h_state_cap = 0;
+        CK(cudaHostAlloc((void **)&ctx->h_state, state, cudaHostAllocDefault));
+        ctx->h_state_cap = state;
+    }
     if (ctx->maxf_cap < 2 * ctx->ntraits) {
         if (ctx->d_maxf) cudaFree(ctx->d_maxf);
         ctx->d_maxf = nullptr;
@@ -497,6 +552,15 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
                              ctx->d_qd + (size_t)ctx->ntraits * ctx->Np, ctx->Np, ctx->ntraits, ctx->d_qm,
                              ctx->d_qm + tn, ctx->stream));
         ctx->qm_valid = true;
+    }
+    if (r.form == EPI_FORM_POPC && !ctx->pm_valid) {
+        const size_t tn = (size_t)ctx->ntraits * ctx->nsnp;
+        CK(ensure(&ctx->d_pmC, &ctx->pmC_cap, 3 * tn * sizeof(double)));
+        CK(ensure(&ctx->d_pmN, &ctx->pmN_cap, 3 * tn * sizeof(int32_t)));
+        CK(ensure(&ctx->d_pmQ, &ctx->pmQ_cap, tn * sizeof(double)));
+        CK(epi::launch_marg(ctx->d_planes, ctx->nsnp, ctx->Wp, ctx->d_y, ctx->d_wmask, ctx->Np, ctx->ntraits,
+                            ctx->d_pmC, ctx->d_pmN, ctx->d_pmQ, ctx->stream));
+        ctx->pm_valid = true;
     }
     epi::ScanArgs &a = r.args;
     memset(&a, 0, sizeof(a));
@@ -515,6 +579,11 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     a.qm = ctx->d_qm;
     a.rm = ctx->d_qm + (size_t)ctx->ntraits * ctx->nsnp;
     a.ydig = ctx->d_ydig;
+    a.maj = ctx->d_maj;
+    a.pmC = ctx->d_pmC;
+    a.pmN = ctx->d_pmN;
+    a.pmQ = ctx->d_pmQ;
+    a.ysq = ctx->d_ysq;
     a.y = ctx->d_y;
     a.q = ctx->d_q;
     a.wmask = ctx->d_wmask;
@@ -537,27 +606,93 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     return EPI_OK;
 }
 
-// Resets the counters and maxima, launches the selected form between the timing events.
-epi_status launch_run(epi_ctx *ctx, ScanRun &r)
+// The device part of a scan, on the context's stream and nothing but stream operations (so it
+// can be captured): counters and maxima reset, the block schedule uploaded from pinned memory,
+// the selected form's persistent kernel between the timing events, and the counters and maxima
+// read back into pinned memory.
+cudaError_t enqueue_scan(epi_ctx *ctx, const ScanRun &r, int grid, int nblocks, bool capturing)
 {
-    CK(cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(unsigned long long), ctx->stream));
-    std::vector<unsigned int> init(2 * ctx->ntraits, 0x007fffffu);  // order-encoded -inf
-    CK(cudaMemcpyAsync(ctx->d_maxf, init.data(), init.size() * sizeof(unsigned int), cudaMemcpyHostToDevice,
-                       ctx->stream));
-    CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    ctx->last_launches = 0;
-    ctx->last_form = r.form;
+    cudaStream_t s = ctx->stream;
+    // under stream capture the timing events are recorded as external records, which become
+    // event nodes of the graph (so they time every replay); a direct launch records them plainly
+    const unsigned int ev_flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    epi::k_scan_init<<<1, 256, 0, s>>>(ctx->d_counters, ctx->d_maxf, 2 * ctx->ntraits);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && nblocks)
+        e = cudaMemcpyAsync(ctx->d_blocks, ctx->h_blocks, nblocks * sizeof(BlockDesc), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev0, s, ev_flags);
+    if (e == cudaSuccess && r.ntiles > 0)
+        e = r.form == EPI_FORM_TENSOR ? epi::mma_enqueue(r.args, ctx->maps, grid, s)
+                                      : epi::popc_enqueue(r.args, ctx->pmaps, grid, s);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev1, s, ev_flags);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ctx->h_state, ctx->d_counters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ctx->h_state + 4, ctx->d_maxf, 2 * (size_t)ctx->ntraits * sizeof(unsigned int),
+                            cudaMemcpyDeviceToHost, s);
+    return e;
+}
+
+template <class T>
+static void key_add(std::vector<unsigned char> &k, const T &v)
+{
+    const unsigned char *p = reinterpret_cast<const unsigned char *>(&v);
+    k.insert(k.end(), p, p + sizeof(T));
+}
+
+// Runs the device part of a scan. With use_graph, a repeat of the previous scan's shape (same
+// kernel arguments, tensor maps, schedule and launch shape) replays the CUDA graph captured for
+// it with one launch; any other scan is captured anew first. Without, the operations are
+// launched one by one.
+epi_status launch_run(epi_ctx *ctx, ScanRun &r, int nblocks, bool use_graph)
+{
+    int grid = 0;
     if (r.ntiles > 0) {
+        const int64_t units = r.ntiles * (int64_t)ctx->ntraits;
         if (r.form == EPI_FORM_TENSOR) {
             // one CTA pair per unit (tile x trait) up to every SM
-            const int64_t units = r.ntiles * (int64_t)ctx->ntraits;
-            CK(epi::launch_mma(r.args, ctx->maps, (int)std::min<int64_t>(2 * units, ctx->sm_count), ctx->stream));
+            CK(epi::mma_prepare(ctx->ntraits, (int)std::min<int64_t>(2 * units, ctx->sm_count), &grid));
         } else {
-            CK(epi::launch_popc(r.args, (int)std::min<int64_t>(r.ntiles, ctx->sm_count), ctx->stream));
+            // one CTA per unit up to every SM
+            CK(epi::popc_prepare());
+            grid = (int)std::min<int64_t>(units, ctx->sm_count);
         }
-        ctx->last_launches = 1;
     }
-    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    if (nblocks) memcpy(ctx->h_blocks, r.desc.data(), nblocks * sizeof(BlockDesc));
+    ctx->last_launches = r.ntiles > 0 ? 2 : 1;  // the state reset and the scan kernel
+    ctx->last_form = r.form;
+    if (!use_graph) {
+        CK(enqueue_scan(ctx, r, grid, nblocks, false));
+        return EPI_OK;
+    }
+    std::vector<unsigned char> key;
+    key_add(key, r.args);
+    key_add(key, r.form);
+    key_add(key, grid);
+    key_add(key, ctx->ntraits);
+    if (r.form == EPI_FORM_TENSOR) key_add(key, ctx->maps);
+    else key_add(key, ctx->pmaps);
+    key.insert(key.end(), reinterpret_cast<const unsigned char *>(r.desc.data()),
+               reinterpret_cast<const unsigned char *>(r.desc.data() + nblocks));
+    if (!ctx->gexec || key != ctx->gkey) {
+        if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+        ctx->gexec = nullptr;
+        ctx->gkey.clear();
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t e = enqueue_scan(ctx, r, grid, nblocks, true);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &g);  // ends the capture in any case
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            CK(e != cudaSuccess ? e : e2);
+        }
+        const cudaError_t e3 = cudaGraphInstantiate(&ctx->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) ctx->gexec = nullptr;
+        CK(e3);
+        ctx->gkey = std::move(key);
+    }
+    CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
     return EPI_OK;
 }
 
@@ -593,11 +728,11 @@ extern "C" epi_status epi_scan(epi_ctx *ctx, const epi_block *blocks, int32_t nb
     for (int attempt = 0; attempt < 2; ++attempt) {
         r.args.hits = ctx->d_hits;
         r.args.cap = ctx->hit_cap;
-        s = launch_run(ctx, r);
+        // the rescan after a regrow is launched directly (a one-off shape)
+        s = launch_run(ctx, r, nblocks, !opts->no_graph && attempt == 0);
         if (s != EPI_OK) return s;
-        unsigned long long cnt[4];
-        CK(cudaMemcpyAsync(cnt, ctx->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        const unsigned long long *cnt = ctx->h_state;
         if (cnt[2] != 0)
             return set_err(ctx, EPI_E_TIMEOUT, "a bounded device wait of the scan kernel gave up (site %llu)",
                            cnt[3]);
@@ -617,14 +752,13 @@ extern "C" epi_status epi_scan(epi_ctx *ctx, const epi_block *blocks, int32_t nb
     for (int b = 0; b < nblocks; ++b) pairs += block_pairs(blocks[b]);
     ctx->last_pairs = pairs * ctx->ntraits;
 
-    std::vector<unsigned int> mx(2 * ctx->ntraits);
-    CK(cudaMemcpyAsync(mx.data(), ctx->d_maxf, mx.size() * sizeof(unsigned int), cudaMemcpyDeviceToHost,
-                       ctx->stream));
+    const unsigned int *mx = reinterpret_cast<const unsigned int *>(ctx->h_state + 4);
     std::vector<DevHit> dh((size_t)found);
-    if (found)
+    if (found) {
         CK(cudaMemcpyAsync(dh.data(), ctx->d_hits, (size_t)found * sizeof(DevHit), cudaMemcpyDeviceToHost,
                            ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
     for (int t = 0; t < ctx->ntraits; ++t) {
         if (max_f) max_f[t] = epi::ord2f(mx[t]);
         if (max_f2) max_f2[t] = opts->test == 'i' ? epi::ord2f(mx[ctx->ntraits + t]) : 0.0f;
@@ -711,14 +845,13 @@ extern "C" epi_status epi_scan_dump(epi_ctx *ctx, const epi_block *block, const 
         r.args.dump_df2 = dd2;
         r.args.hits = ctx->d_hits;
         r.args.cap = 0;
-        st = launch_run(ctx, r);
+        st = launch_run(ctx, r, 1, false);
     }
     if (st == EPI_OK) {
-        unsigned long long cnt[4];
-        cudaError_t e = cudaMemcpyAsync(cnt, ctx->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) st = set_err(ctx, EPI_E_CUDA, "dump: %s", cudaGetErrorString(e));
-        else if (cnt[2] != 0) st = set_err(ctx, EPI_E_TIMEOUT, "a bounded device wait gave up (site %llu)", cnt[3]);
+        else if (ctx->h_state[2] != 0)
+            st = set_err(ctx, EPI_E_TIMEOUT, "a bounded device wait gave up (site %llu)", ctx->h_state[3]);
     }
     if (st == EPI_OK) {
         for (Out &x : outs) {

@@ -8,6 +8,9 @@
 //   y       float [T][Np]         trait column centred by its valid mean, 0 where invalid
 //   q       float [T][Np]         y^2 - qc[t] (qc = mean of y^2 over valid), 0 where invalid
 //   wmask   uint32 [T][Wp]        phenotype-valid bits
+//   maj     uint8 [nsnp]          most frequent genotype of each SNP (plain form)
+//   pmC, pmN, pmQ                 plain form: per (trait, SNP) the sums of y and the counts by
+//                                 genotype, and the sum of y^2 over the SNP's missing calls
 // and for the tensor-core form
 //   hcodes  uint8 [nsnp][Np]      one-hot genotype byte: 1 << g for g in 0..2, 0 if missing
 //   missbits uint32 [nsnp][Wp]    missing-genotype bits
@@ -74,6 +77,13 @@ struct ScanArgs {
     const double *qd, *qtot, *qm, *rm;
     const double *qcen, *qstep;  // [T] (tensor form: centre and step of the 16-bit y^2 digits)
     const int8_t *ydig;
+    // plain form: per SNP the most frequent genotype; per (trait, SNP) the FP64 marginals by
+    // genotype -- sum of y [T][nsnp][3], count [T][nsnp][3], sum of y^2 over the individuals
+    // missing at the SNP [T][nsnp] -- and per trait the sum of y^2 over valid individuals
+    const uint8_t *maj;
+    const double *pmC;
+    const int32_t *pmN;
+    const double *pmQ, *ysq;
     int32_t Np, ntraits;
     // blocks / tiles
     const BlockDesc *blocks;
@@ -105,6 +115,11 @@ struct ScanArgs {
 // TMA descriptors of the tensor form (kernel parameter, __grid_constant__)
 struct MmaMaps {
     CUtensorMap hi, hj, dg;
+};
+
+// TMA descriptor of the plain form: the genotype plane words
+struct PopcMaps {
+    CUtensorMap planes;
 };
 
 // float -> unsigned with the same order (for atomicMax over possibly negative F)

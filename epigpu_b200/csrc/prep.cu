@@ -94,6 +94,101 @@ __global__ void k_qmiss(const uint32_t *__restrict__ missbits, int nsnp, int Wp,
     if (rm) rm[gid] = r;
 }
 
+// Per SNP the most frequent genotype (ties to the lower code), one warp per SNP: the plain
+// form derives that genotype's row of the 3x3 table from the SNP's marginals.
+__global__ void k_major(const uint4 *__restrict__ planes, int nsnp, int Wp, uint8_t *__restrict__ maj)
+{
+    const long long s = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (s >= nsnp) return;
+    int c0 = 0, c1 = 0, c2 = 0;
+    for (int w = lane; w < Wp; w += 32) {
+        const uint4 P = planes[(size_t)s * Wp + w];
+        c0 += __popc(P.x);
+        c1 += __popc(P.y);
+        c2 += __popc(P.z);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+        c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+        c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+    }
+    if (lane == 0) maj[s] = (uint8_t)((c0 >= c1 && c0 >= c2) ? 0 : (c1 >= c2 ? 1 : 2));
+}
+
+// Plain-form marginals, one warp per (trait t, SNP s), lane = individual within each 32-word:
+// pmC[t][s][b] = sum of y over g_s = b, pmN[t][s][b] = number of phenotype-valid individuals
+// with g_s = b, pmQ[t][s] = sum of y^2 over the valid individuals missing at s. FP64 per lane,
+// then a warp-shuffle reduction.
+__global__ void k_marg(const uint4 *__restrict__ planes, int nsnp, int Wp, const float *__restrict__ y,
+                       const uint32_t *__restrict__ wmask, int Np, int ntraits, double *__restrict__ pmC,
+                       int32_t *__restrict__ pmN, double *__restrict__ pmQ)
+{
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw >= (long long)nsnp * ntraits) return;
+    const int t = (int)(gw / nsnp), s = (int)(gw % nsnp);
+    double c0 = 0.0, c1 = 0.0, c2 = 0.0, q = 0.0;
+    int n0 = 0, n1 = 0, n2 = 0;
+    const float *yt = y + (size_t)t * Np;
+    const uint32_t *wt = wmask + (size_t)t * Wp;
+    for (int w = 0; w < Wp; ++w) {
+        const uint4 P = planes[(size_t)s * Wp + w];
+        const uint32_t W = wt[w];
+        const double yv = (double)yt[32 * w + lane];
+        const int ok = (W >> lane) & 1u;
+        if ((P.x >> lane) & 1u) {
+            c0 += yv;
+            n0 += ok;
+        } else if ((P.y >> lane) & 1u) {
+            c1 += yv;
+            n1 += ok;
+        } else if ((P.z >> lane) & 1u) {
+            c2 += yv;
+            n2 += ok;
+        } else if (ok) {
+            q += yv * yv;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+        c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+        c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+        q += __shfl_xor_sync(0xffffffffu, q, o);
+        n0 += __shfl_xor_sync(0xffffffffu, n0, o);
+        n1 += __shfl_xor_sync(0xffffffffu, n1, o);
+        n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+    }
+    if (lane == 0) {
+        const size_t o = (size_t)gw;
+        pmC[3 * o] = c0;
+        pmC[3 * o + 1] = c1;
+        pmC[3 * o + 2] = c2;
+        pmN[3 * o] = n0;
+        pmN[3 * o + 1] = n1;
+        pmN[3 * o + 2] = n2;
+        pmQ[o] = q;
+    }
+}
+
+cudaError_t launch_major(const uint4 *planes, int nsnp, int Wp, uint8_t *maj, cudaStream_t stream)
+{
+    const long long threads = 32LL * nsnp;
+    k_major<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(planes, nsnp, Wp, maj);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_marg(const uint4 *planes, int nsnp, int Wp, const float *y, const uint32_t *wmask, int Np,
+                        int ntraits, double *pmC, int32_t *pmN, double *pmQ, cudaStream_t stream)
+{
+    const long long threads = 32LL * nsnp * ntraits;
+    k_marg<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(planes, nsnp, Wp, y, wmask, Np, ntraits, pmC, pmN,
+                                                                 pmQ);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int remain, uint4 *planes, int Wp,
                           uint32_t *codes, int Wc, uint8_t *hcodes, uint8_t *h3, uint32_t *missbits,
                           cudaStream_t stream)

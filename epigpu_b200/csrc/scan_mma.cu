@@ -831,33 +831,40 @@ struct MmaShape {
 static std::mutex g_shape_mu;
 static std::vector<MmaShape> g_shapes;
 
-cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream)
+static cudaLaunchConfig_t mma_config(int ntraits, int grid, cudaStream_t stream, cudaLaunchAttribute *attr)
 {
-    // more than half of the SM's shared memory: one CTA per SM, which owns all 512 TMEM
-    // columns; the tail holds the per-CTA maxima. CTAs run in clusters of two (the pair MMA).
-    const size_t smem = sizeof(mma::Smem) + 1024 + smax_bytes(a.ntraits);
-    static_assert(sizeof(mma::Smem) + 1024 > 116 * 1024, "one CTA per SM");
-    int device = 0;
-    cudaError_t e = cudaGetDevice(&device);
-    if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = 2;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    // whole clusters of two: at least one, and never more than can be resident at once
-    cfg.gridDim = dim3((unsigned)std::max(2, (grid + 1) & ~1), 1, 1);
+    cfg.gridDim = dim3((unsigned)grid, 1, 1);
     cfg.blockDim = dim3(mma::NTHREADS, 1, 1);
-    cfg.dynamicSmemBytes = smem;
+    // more than half of the SM's shared memory: one CTA per SM, which owns all 512 TMEM
+    // columns; the tail holds the per-CTA maxima
+    cfg.dynamicSmemBytes = sizeof(mma::Smem) + 1024 + smax_bytes(ntraits);
     cfg.stream = stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    return cfg;
+}
+
+// The launch shape of a scan, resolved before any stream capture: the kernel's shared-memory
+// attribute and the number of co-resident clusters (queried once per device and size), then
+// whole clusters of two -- at least one, never more than can be resident at once.
+cudaError_t mma_prepare(int ntraits, int grid_request, int *grid)
+{
+    static_assert(sizeof(mma::Smem) + 1024 > 116 * 1024, "one CTA per SM");
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = mma_config(ntraits, std::max(2, (grid_request + 1) & ~1), nullptr, attr);
     int clusters = 0;
     {
         std::lock_guard<std::mutex> lock(g_shape_mu);
         for (const MmaShape &sh : g_shapes)
-            if (sh.device == device && sh.smem == smem) clusters = sh.clusters;
+            if (sh.device == device && sh.smem == cfg.dynamicSmemBytes) clusters = sh.clusters;
         if (clusters == 0) {
             // the attribute admits the largest size any trait count asks for
             e = cudaFuncSetAttribute(mma::k_scan_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -866,11 +873,19 @@ cudaError_t launch_mma(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStr
             e = cudaOccupancyMaxActiveClusters(&clusters, mma::k_scan_mma, &cfg);
             if (e != cudaSuccess) return e;
             if (clusters < 1) return cudaErrorInvalidConfiguration;
-            g_shapes.push_back({device, smem, clusters});
+            g_shapes.push_back({device, cfg.dynamicSmemBytes, clusters});
         }
     }
-    if (2 * clusters < (int)cfg.gridDim.x) cfg.gridDim.x = 2 * (unsigned)clusters;
-    e = cudaLaunchKernelEx(&cfg, mma::k_scan_mma, a, maps);
+    *grid = std::min((int)cfg.gridDim.x, 2 * clusters);
+    return cudaSuccess;
+}
+
+// The launch itself (a stream operation only, so it can be captured into a CUDA graph).
+cudaError_t mma_enqueue(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream)
+{
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = mma_config(a.ntraits, grid, stream, attr);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, mma::k_scan_mma, a, maps);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }

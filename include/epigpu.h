@@ -74,7 +74,10 @@ typedef struct epi_scan_opts {
     int32_t debug;         /* 0; EPI_DEBUG_STALL (tests of the timeout path only): one wait of
                             * the tensor form is on a barrier nothing arrives at, so it runs
                             * out after wait_limit_ms and the scan returns EPI_E_TIMEOUT */
-    int32_t reserved[7];   /* set to 0 */
+    int32_t no_graph;      /* 0: the scan's device work is captured as a CUDA graph and a repeat of
+                            * the same scan shape (kernel arguments, blocks) replays it with one
+                            * launch; 1: every operation is launched directly */
+    int32_t reserved[6];   /* set to 0 */
 } epi_scan_opts;
 
 #define EPI_DEBUG_STALL 1
