@@ -5,21 +5,25 @@
 // Persistent kernel, one 512-thread CTA per SM, pulling (64 x 64 SNP-pair tile, trait) units
 // from a queue over the tile schedule of the chromosome blocks. The genotype bit-plane words of
 // the tile's 64 i-SNPs and 64 j-SNPs (planes of g==0, g==1, g==2, g!=3 per 32 individuals)
-// arrive by TMA, 64 individuals per stage, in a three-stage ring. Per stage:
-//   * expansion (all threads, double-buffered): for each i-SNP the two genotypes other than
-//     its most frequent one, A and B, become U_A = [g_i==A]*y and U_B = [g_i==B]*y floats in
-//     shared memory, with the phenotype-masked plane words of A and B and of the missing calls;
-//   * cell counts n_Ab, n_Bb: AND + __popc of 32-bit plane words, 16-bit packed counters;
-//   * cell sums S_Ab, S_Bb: each lane holds its own j-SNP's plane words and adds the warp's
-//     broadcast U values into the cells its genotype bits select (6 FP32 adds per pair and
-//     individual, predicated by the bits: no 0/1 multiplications);
+// arrive by TMA, 64 individuals per stage, in a three-stage ring. Each SNP's two genotypes
+// other than its most frequent one are its dense genotypes A and B. Per stage:
+//   * expansion (all threads, double-buffered): for each i-SNP, U_A = [g_i==A]*y and
+//     U_B = [g_i==B]*y floats in shared memory, with the phenotype-masked plane words of A, B
+//     and of the missing calls;
+//   * cell counts of the dense 2x2 cells and of the individuals missing at j: AND + __popc of
+//     32-bit plane words, 16-bit packed counters;
+//   * cell sums S_{Ai,Aj}, S_{Ai,Bj}, S_{Bi,Aj}, S_{Bi,Bj}: each lane holds its own j-SNP's
+//     plane words and adds the warp's broadcast U values into the cells its genotype bits
+//     select (4 FP32 adds per pair and individual, predicated by the bits);
+//   * individuals missing at the j-SNP (per lane, sparse): their sums by the i genotype;
 //   * individuals missing at the i-SNP (warp-uniform, sparse): their sums and counts by the
 //     j genotype, and the sum of y^2 of individuals missing at both SNPs.
-// The third row and the sum of squares come from per-(trait, SNP) FP64 marginals in the
-// epilogue: S_Mb = C_b(j) - S_Ab - S_Bb - S_3b (C_b(j) = sum of y over g_j = b), likewise
-// the counts, and Q = Qtot - QM_i - QM_j + QMM. Deriving the most frequent genotype's row
-// keeps the FP32 sums to the smaller cells. Each thread owns 8 whole pairs (the warp's 8
-// i-SNPs x the lane's j-SNP), so the reduction over individuals stays in registers.
+// The most frequent genotypes' row and column and the sum of squares come from per-(trait,
+// SNP) FP64 marginals in the epilogue: S_{a,Mj} = R_a(i) - S_{a,Aj} - S_{a,Bj} - S_{a,3}
+// (R_a(i) = sum of y over g_i = a), then S_{Mi,b} = C_b(j) - S_{Ai,b} - S_{Bi,b} - S_{3,b},
+// likewise the counts, and Q = Qtot - QM_i - QM_j + QMM. Deriving the most frequent
+// genotypes keeps the FP32 sums to the smaller cells. Each thread owns 8 whole pairs (the
+// warp's 8 i-SNPs x the lane's j-SNP), so the reduction over individuals stays in registers.
 // Epilogue: FP64 SSB/SSI/F/F2 per pair (src/EpiOpenCL.c:231-247, :452-486), warp-aggregated
 // atomic hit append, per-trait maxima (warp-shuffle reductions).
 #include <cuda.h>
@@ -48,23 +52,26 @@ struct Smem {
     uint4 raw_i[RS][TI][KW];  // TMA: plane words of the i-tile (row = SNP)
     uint4 raw_j[RS][TJ][KW];  // TMA: plane words of the j-tile
     float4 u[2][KP][TI];      // (U_A(k), U_A(k+1), U_B(k), U_B(k+1)) of each i-SNP
-    uint4 pm[2][KW][TI];      // (P_A & W, P_B & W, missing & W, 0) of each i-SNP
+    uint4 pm[2][KW][TI];      // (P_A & W, P_B & W, missing & W, W) of each i-SNP
     float y[2][KI];           // the stage's trait values (0 where invalid)
     float4 sps[PI][NT];       // per pair: sums over individuals missing at i by g_j: S_30..S_32, QMM
     uint2 spn[PI][NT];        // and counts: n_30 | n_31 << 16, n_32
+    float2 spj[PI][NT];       // per pair: sums over individuals missing at j by g_i: S_{Ai,3}, S_{Bi,3}
     uint64_t full[RS];
-    uint8_t maj[TI];
+    uint8_t maj[TI];          // most frequent genotype of each i-SNP
+    uint8_t majj[TJ];         // and of each j-SNP
     long long unit;
     int never;                // always 0: the abort flag of the bounded waits
 };
 
 // One pair's accumulators and the per-SNP values its statistics need, passed out of line.
 struct PairIn {
-    float SA[3], SB[3];
-    uint32_t C[3];
-    float4 sp;
-    uint2 spn;
-    int maj, trait, si, sj, gi, gj, size2;
+    float S[4];    // S_{Ai,Aj}, S_{Ai,Bj}, S_{Bi,Aj}, S_{Bi,Bj}
+    float SJ[2];   // S_{Ai,3}, S_{Bi,3}: individuals missing at j
+    uint32_t C[3]; // n_{Ai,Aj} | n_{Ai,Bj} << 16, n_{Bi,Aj} | n_{Bi,Bj} << 16, n_{Ai,3} | n_{Bi,3} << 16
+    float4 sp;     // individuals missing at i, by g_j: S_{3,0..2}, and QMM
+    uint2 spn;     // n_{3,0} | n_{3,1} << 16, n_{3,2}
+    int maj, majj, trait, si, sj, gi, gj, size2;
 };
 
 // FP64 statistics of one pair: the most frequent genotype's row from the marginals, then the
@@ -72,24 +79,41 @@ struct PairIn {
 // kernel's accumulators stay in registers.
 __device__ __noinline__ PairStat eval_pair(const ScanArgs &a, const PairIn p)
 {
-    const int A = p.maj == 0 ? 1 : 0, B = p.maj == 2 ? 1 : 2, M = p.maj;
-    const int nA[3] = {(int)(p.C[0] & 0xffffu), (int)(p.C[0] >> 16), (int)(p.C[1] & 0xffffu)};
-    const int nB[3] = {(int)(p.C[1] >> 16), (int)(p.C[2] & 0xffffu), (int)(p.C[2] >> 16)};
-    const int n3[3] = {(int)(p.spn.x & 0xffffu), (int)(p.spn.x >> 16), (int)p.spn.y};
-    const double S3[3] = {(double)p.sp.x, (double)p.sp.y, (double)p.sp.z};
-    const size_t mj = (size_t)p.trait * a.nsnp + p.sj;
+    const int Ai = p.maj == 0 ? 1 : 0, Bi = p.maj == 2 ? 1 : 2, Mi = p.maj;
+    const int Aj = p.majj == 0 ? 1 : 0, Bj = p.majj == 2 ? 1 : 2, Mj = p.majj;
+    const size_t mi = (size_t)p.trait * a.nsnp + p.si, mj = (size_t)p.trait * a.nsnp + p.sj;
     int n[9];
     double S[9];
+    // the dense 2 x 2 cells
+    n[3 * Ai + Aj] = (int)(p.C[0] & 0xffffu);
+    n[3 * Ai + Bj] = (int)(p.C[0] >> 16);
+    n[3 * Bi + Aj] = (int)(p.C[1] & 0xffffu);
+    n[3 * Bi + Bj] = (int)(p.C[1] >> 16);
+    S[3 * Ai + Aj] = (double)p.S[0];
+    S[3 * Ai + Bj] = (double)p.S[1];
+    S[3 * Bi + Aj] = (double)p.S[2];
+    S[3 * Bi + Bj] = (double)p.S[3];
+    // the j-SNP's most frequent genotype, rows Ai and Bi: the i-SNP's marginal less the row's
+    // other cells and its individuals missing at j
+    n[3 * Ai + Mj] = a.pmN[3 * mi + Ai] - n[3 * Ai + Aj] - n[3 * Ai + Bj] - (int)(p.C[2] & 0xffffu);
+    n[3 * Bi + Mj] = a.pmN[3 * mi + Bi] - n[3 * Bi + Aj] - n[3 * Bi + Bj] - (int)(p.C[2] >> 16);
+    S[3 * Ai + Mj] = a.pmC[3 * mi + Ai] - S[3 * Ai + Aj] - S[3 * Ai + Bj] - (double)p.SJ[0];
+    S[3 * Bi + Mj] = a.pmC[3 * mi + Bi] - S[3 * Bi + Aj] - S[3 * Bi + Bj] - (double)p.SJ[1];
+    // the i-SNP's most frequent genotype, every column: the j-SNP's marginal less the column's
+    // other cells and its individuals missing at i
+    const int n3[3] = {(int)(p.spn.x & 0xffffu), (int)(p.spn.x >> 16), (int)p.spn.y};
+    const double S3[3] = {(double)p.sp.x, (double)p.sp.y, (double)p.sp.z};
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
-        n[3 * A + b] = nA[b];
-        n[3 * B + b] = nB[b];
-        n[3 * M + b] = a.pmN[3 * mj + b] - nA[b] - nB[b] - n3[b];
-        S[3 * A + b] = (double)p.SA[b];
-        S[3 * B + b] = (double)p.SB[b];
-        S[3 * M + b] = a.pmC[3 * mj + b] - (double)p.SA[b] - (double)p.SB[b] - S3[b];
+        n[3 * Mi + b] = a.pmN[3 * mj + b] - n[3 * Ai + b] - n[3 * Bi + b] - n3[b];
+        S[3 * Mi + b] = a.pmC[3 * mj + b] - S[3 * Ai + b] - S[3 * Bi + b] - S3[b];
     }
-    const double Qv = a.ysq[p.trait] - a.pmQ[(size_t)p.trait * a.nsnp + p.si] - a.pmQ[mj] + (double)p.sp.w;
+    // an empty cell's sum is 0: a derived sum of an empty cell holds only the rounding of the
+    // FP32 sums it was formed from (so a pair without valid individuals keeps F = 0/0 = NaN)
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+        if (n[c] == 0) S[c] = 0.0;
+    const double Qv = a.ysq[p.trait] - a.pmQ[mi] - a.pmQ[mj] + (double)p.sp.w;
     const PairStat s = pair_stat(n, S, Qv, a.test_int != 0);
     if (p.trait == a.report_trait) {
         const size_t o = (size_t)p.gi * p.size2 + p.gj;
@@ -162,10 +186,13 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a, const __grid_co
         const float *yt = a.y + (size_t)t * a.Np;
         const uint32_t *wt = a.wmask + (size_t)t * a.Wp;
         if (tid < TI) sm.maj[tid] = i0 + tid < bd.size1 ? a.maj[bd.start1 + i0 + tid] : (uint8_t)0;
+        else if (tid < TI + TJ)
+            sm.majj[tid - TI] = j0 + tid - TI < bd.size2 ? a.maj[bd.start2 + j0 + tid - TI] : (uint8_t)0;
 #pragma unroll
         for (int ii = 0; ii < PI; ++ii) {
             sm.sps[ii][tid] = make_float4(0.f, 0.f, 0.f, 0.f);
             sm.spn[ii][tid] = make_uint2(0u, 0u);
+            sm.spj[ii][tid] = make_float2(0.f, 0.f);
         }
         auto issue = [&](int st) {  // thread 0: the TMA loads of stage st
             const int r = st % RS;
@@ -202,7 +229,7 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a, const __grid_co
                 const int mj = sm.maj[i];
                 const uint32_t W = __ldg(wt + KW * st + w);
                 const uint32_t PA = mj == 0 ? P.y : P.x, PB = mj == 2 ? P.y : P.z;
-                sm.pm[b][w][i] = make_uint4(PA & W, PB & W, ~P.w & W, 0u);
+                sm.pm[b][w][i] = make_uint4(PA & W, PB & W, ~P.w & W, W);
             } else if (tid < TI * KW + KI / 4) {
                 const int q = tid - TI * KW;
                 reinterpret_cast<float4 *>(sm.y[b])[q] = __ldg(reinterpret_cast<const float4 *>(yt + KI * st) + q);
@@ -213,14 +240,15 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a, const __grid_co
         expand(0, 0);
         __syncthreads();
 
-        float S[PI][6];
+        float S[PI][4];
         uint32_t C[PI][3];
 #pragma unroll
         for (int ii = 0; ii < PI; ++ii) {
 #pragma unroll
-            for (int c = 0; c < 6; ++c) S[ii][c] = 0.f;
+            for (int c = 0; c < 4; ++c) S[ii][c] = 0.f;
             C[ii][0] = C[ii][1] = C[ii][2] = 0u;
         }
+        const int mjj = sm.majj[jl];  // this lane's j-SNP: its dense genotypes' planes
 
         for (int st = 0; st < nst; ++st) {
             const int b = st & 1, r = st % RS;
@@ -231,13 +259,14 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a, const __grid_co
 #pragma unroll 1
             for (int w = 0; w < KW; ++w) {
                 const uint4 pj = sm.raw_j[r][jl][w];
+                const uint32_t PAj = mjj == 0 ? pj.y : pj.x, PBj = mjj == 2 ? pj.y : pj.z, Mj = ~pj.w;
                 // counts and the sparse individuals missing at i
 #pragma unroll
                 for (int ii = 0; ii < PI; ++ii) {
                     const uint4 pm = sm.pm[b][w][ib + ii];
-                    C[ii][0] += __popc(pm.x & pj.x) + (__popc(pm.x & pj.y) << 16);
-                    C[ii][1] += __popc(pm.x & pj.z) + (__popc(pm.y & pj.x) << 16);
-                    C[ii][2] += __popc(pm.y & pj.y) + (__popc(pm.y & pj.z) << 16);
+                    C[ii][0] += __popc(pm.x & PAj) + (__popc(pm.x & PBj) << 16);
+                    C[ii][1] += __popc(pm.y & PAj) + (__popc(pm.y & PBj) << 16);
+                    C[ii][2] += __popc(pm.x & Mj) + (__popc(pm.y & Mj) << 16);
                     uint32_t m = pm.z;  // the same in every lane of the warp
                     while (m) {
                         const int k = __ffs(m) - 1;
@@ -256,27 +285,38 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a, const __grid_co
                         sm.spn[ii][tid] = nn;
                     }
                 }
+                // individuals missing at this lane's j-SNP (and phenotype-valid): their sums by
+                // the i genotype (per lane; rare)
+                uint32_t mj = Mj & sm.pm[b][w][ib].w;
+                while (mj) {
+                    const int k = __ffs(mj) - 1;
+                    mj &= mj - 1u;
+                    const float yv = sm.y[b][32 * w + k];
+#pragma unroll
+                    for (int ii = 0; ii < PI; ++ii) {
+                        const uint2 pab = *reinterpret_cast<const uint2 *>(&sm.pm[b][w][ib + ii]);
+                        float2 acc = sm.spj[ii][tid];
+                        acc.x += bit(pab.x, k) ? yv : 0.f;
+                        acc.y += bit(pab.y, k) ? yv : 0.f;
+                        sm.spj[ii][tid] = acc;
+                    }
+                }
                 // sums: this lane's j genotype bits select the cells the U values go to
 #pragma unroll
                 for (int h = 0; h < 16; ++h) {
                     const int k = 2 * h;
-                    const bool f0a = bit(pj.x, k), f1a = bit(pj.y, k), f2a = bit(pj.z, k);
-                    const bool f0b = bit(pj.x, k + 1), f1b = bit(pj.y, k + 1), f2b = bit(pj.z, k + 1);
+                    const bool fAa = bit(PAj, k), fBa = bit(PBj, k), fAb = bit(PAj, k + 1), fBb = bit(PBj, k + 1);
 #pragma unroll
                     for (int ii = 0; ii < PI; ++ii) {
                         const float4 uu = sm.u[b][16 * w + h][ib + ii];
-                        if (f0a) S[ii][0] += uu.x;
-                        if (f1a) S[ii][1] += uu.x;
-                        if (f2a) S[ii][2] += uu.x;
-                        if (f0a) S[ii][3] += uu.z;
-                        if (f1a) S[ii][4] += uu.z;
-                        if (f2a) S[ii][5] += uu.z;
-                        if (f0b) S[ii][0] += uu.y;
-                        if (f1b) S[ii][1] += uu.y;
-                        if (f2b) S[ii][2] += uu.y;
-                        if (f0b) S[ii][3] += uu.w;
-                        if (f1b) S[ii][4] += uu.w;
-                        if (f2b) S[ii][5] += uu.w;
+                        if (fAa) S[ii][0] += uu.x;
+                        if (fBa) S[ii][1] += uu.x;
+                        if (fAa) S[ii][2] += uu.z;
+                        if (fBa) S[ii][3] += uu.z;
+                        if (fAb) S[ii][0] += uu.y;
+                        if (fBb) S[ii][1] += uu.y;
+                        if (fAb) S[ii][2] += uu.w;
+                        if (fBb) S[ii][3] += uu.w;
                     }
                 }
             }
@@ -297,14 +337,16 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a, const __grid_co
             if (valid) {
                 PairIn p;
 #pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    p.SA[c] = S[ii][c];
-                    p.SB[c] = S[ii][3 + c];
-                    p.C[c] = C[ii][c];
-                }
+                for (int c = 0; c < 4; ++c) p.S[c] = S[ii][c];
+                const float2 sj = sm.spj[ii][tid];
+                p.SJ[0] = sj.x;
+                p.SJ[1] = sj.y;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) p.C[c] = C[ii][c];
                 p.sp = sm.sps[ii][tid];
                 p.spn = sm.spn[ii][tid];
                 p.maj = sm.maj[ib + ii];
+                p.majj = sm.majj[jl];
                 p.trait = t;
                 p.si = bd.start1 + gi;
                 p.sj = bd.start2 + gj;
