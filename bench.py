@@ -402,6 +402,7 @@ def main():
         dev_s = e0.elapsed_time(e1) / 1e3
     dev_s = max_over_ranks(dev_s, pg)
     value = pairs_step * args.steps * world / dev_s
+    kernel_config = ctx.scan_config()
     used_form = "tensor" if used == capi.FORM_TENSOR else "popc"
 
     # end to end through the C ABI from host buffers
@@ -430,7 +431,8 @@ def main():
         ctx.scan(popc_blocks, po, ntraits=ntraits)
         ctx.scan(popc_blocks, po, ntraits=ntraits)
         ms, pp, _, _ = ctx.last_timing()
-        popc = {"value": pp / (ms / 1e3), "unit": "pairs/s", "sample": "%d-SNP triangle" % m}
+        popc = {"value": pp / (ms / 1e3), "unit": "pairs/s", "sample": "%d-SNP triangle" % m,
+                "kernel": ctx.scan_config()}
 
     # planted pairs among the last step's hits (trait 0)
     found = set(zip(hits["snp1"].tolist(), hits["snp2"].tolist()))
@@ -460,13 +462,17 @@ def main():
                     "traffic_source": "ncu dram__bytes_read+write on cfg3m, scaled by pairs x individuals",
                     "peak_source": "cuBLAS int8 GEMM measured in this run (torch._int_mm 8192^3)"}
         else:
-            # plain form: 10 FP32 FMAs per pair and individual (9 cell sums + sum of squares)
-            # against the FP32 FMA issue peak at the sampled SM clock
+            # plain form: 4 FP32 adds per pair and individual (the dense 2 x 2 genotype cells;
+            # the rest of the 3 x 3 table and the sum of squares come from per-SNP marginals)
+            # against the FP32 pipe's peak at the sampled SM clock; beside it, the same rate in
+            # the reference method's 10 FP32 operations per pair and individual (9 cell sums and
+            # the sum of squares, src/EpiOpenCL.c:110-228)
             mhz = clocks["sm_mhz"] or 1965.0
             peak = sms * 128 * mhz * 1e6 / 1e12
-            achieved = pairs_launch * 10.0 * nid / kern_s / 1e12
-            roof = {"bound": "alu", "achieved": achieved, "peak": peak, "unit": "TFMA/s",
+            achieved = pairs_launch * 4.0 * nid / kern_s / 1e12
+            roof = {"bound": "alu", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "traffic": None,
+                    "reference_method_frac": pairs_launch * 10.0 * nid / kern_s / 1e12 / peak,
                     "peak_source": "%d SMs x 128 FP32 lanes x %.0f MHz sampled SM clock" % (sms, mhz)}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -483,7 +489,8 @@ def main():
                        "blocks": len(blocks), "traits": ntraits, "test": test, "t1": t1, "t2": t2,
                        "pairs_per_step": pairs_step, "form": used_form, "hits_per_step": int(nhits),
                        "l2": "inputs larger than L2 (packed genotypes %.0f MB)" % (gp.nbytes / 1e6),
-                       "gpu": gname, "planted": planted, "cuda_graph": not args.no_graph},
+                       "gpu": gname, "planted": planted, "cuda_graph": not args.no_graph,
+                       "kernel": kernel_config},
             "e2e": {"value": pairs_step * args.steps * world / e2e_s, "unit": "pairs/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),

@@ -28,7 +28,7 @@ DEBUG_STALL = 1
 EXPORTS = (
     "epi_default_opts", "epi_open", "epi_close", "epi_strerror", "epi_last_error",
     "epi_device_info", "epi_load_packed", "epi_set_traits", "epi_set_phenotype", "epi_scan",
-    "epi_scan_dump", "epi_last_timing", "epi_get_stream", "epi_scan_block_noalloc", "epi_permute_phenotype",
+    "epi_scan_dump", "epi_last_timing", "epi_scan_config", "epi_get_stream", "epi_scan_block_noalloc", "epi_permute_phenotype",
 )
 
 
@@ -47,7 +47,7 @@ class ScanOpts(ctypes.Structure):
     _fields_ = [("test", ctypes.c_int32), ("safe", ctypes.c_int32), ("chunk", ctypes.c_int32),
                 ("t1", ctypes.c_float), ("t2", ctypes.c_float), ("form", ctypes.c_int32),
                 ("report_trait", ctypes.c_int32), ("wait_limit_ms", ctypes.c_int32), ("debug", ctypes.c_int32),
-                ("no_graph", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
+                ("no_graph", ctypes.c_int32), ("tile_config", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
 
 
 HIT_DTYPE = np.dtype([("snp1", "<i4"), ("snp2", "<i4"), ("df1", "<i4"), ("df2", "<i4"),
@@ -71,6 +71,7 @@ _SIGS = {
     "epi_last_timing": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64),
                                        ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
     "epi_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+    "epi_scan_config": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_int32]),
     "epi_scan_block_noalloc": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _P, ctypes.POINTER(Block),
                                               ctypes.POINTER(ScanOpts), _P, ctypes.c_int64, _P, _P, _P]),
     "epi_permute_phenotype": (None, [_P, ctypes.c_int32, ctypes.c_uint32]),
@@ -108,7 +109,7 @@ def _ptr(a):
 
 
 def default_opts(test="f", safe=0, chunk=128, t1=6.5, t2=10.5, form=FORM_AUTO, report_trait=0, wait_limit_ms=0,
-                 debug=0, no_graph=0):
+                 debug=0, no_graph=0, tile_config=0):
     o = ScanOpts()
     load().epi_default_opts(ctypes.byref(o))
     o.test = ord(test) if isinstance(test, str) else int(test)
@@ -121,6 +122,7 @@ def default_opts(test="f", safe=0, chunk=128, t1=6.5, t2=10.5, form=FORM_AUTO, r
     o.wait_limit_ms = int(wait_limit_ms)
     o.debug = int(debug)
     o.no_graph = int(no_graph)
+    o.tile_config = int(tile_config)
     return o
 
 
@@ -231,6 +233,12 @@ class Context:
                                                _ptr(counts), _ptr(F), _ptr(F2), _ptr(d1), _ptr(d2)),
                         "epi_scan_dump")
         return {"counts": counts, "F": F, "F2": F2, "df1": d1, "df2": d2}
+
+    def scan_config(self):
+        """The form and kernel variant of the last scan and how the variant was chosen."""
+        buf = ctypes.create_string_buffer(512)
+        self._check(self.lib.epi_scan_config(self.h, buf, 512), "epi_scan_config")
+        return buf.value.decode()
 
     def stream_handle(self):
         """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""

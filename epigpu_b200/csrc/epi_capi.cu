@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -28,19 +29,21 @@ cudaError_t launch_major(const uint4 *planes, int nsnp, int Wp, uint8_t *maj, cu
 cudaError_t launch_marg(const uint4 *planes, int nsnp, int Wp, const float *y, const uint32_t *wmask, int Np,
                         int ntraits, double *pmC, int32_t *pmN, double *pmQ, cudaStream_t stream);
 // plain form (scan_popc.cu)
-cudaError_t popc_prepare();
-cudaError_t popc_enqueue(const ScanArgs &a, const PopcMaps &maps, int grid, cudaStream_t stream);
-cudaError_t popc_encode_planes(PopcMaps *maps, const uint4 *planes, int nsnp, int Wp);
-int popc_tile_i();
-int popc_tile_j();
+int popc_shapes();
+void popc_shape(int v, int *ti, int *tj, const char **desc);
+cudaError_t popc_prepare(int v);
+cudaError_t popc_enqueue(int v, const ScanArgs &a, const PopcMaps &maps, int grid, cudaStream_t stream);
+cudaError_t popc_encode_planes(int v, PopcMaps *maps, const uint4 *planes, int nsnp, int Wp);
 // tensor form (scan_mma.cu)
 bool mma_available();
 int mma_tile_i();
 int mma_tile_j();
 int mma_min_nid();
 int mma_max_nid();
-cudaError_t mma_prepare(int ntraits, int grid_request, int *grid);
-cudaError_t mma_enqueue(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream);
+int mma_shapes();
+void mma_shape(int v, const char **desc);
+cudaError_t mma_prepare(int v, int ntraits, int grid_request, int *grid);
+cudaError_t mma_enqueue(int v, const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream);
 cudaError_t mma_encode_genotypes(MmaMaps *maps, const uint8_t *hcodes, const uint8_t *h3, int nsnp, int Np);
 cudaError_t mma_encode_traits(MmaMaps *maps, const int8_t *ydig, int ntraits, int Np);
 // Start of a scan: counters (hits, tile queue, error flag and site) to zero, the per-trait
@@ -110,6 +113,7 @@ struct epi_ctx {
     int64_t last_pairs = 0;
     int last_launches = 0;
     int last_form = 0;
+    std::string last_config;  // form, kernel variant and how it was chosen
     std::string err;
 };
 
@@ -264,7 +268,6 @@ epi_status epi_load_packed(epi_ctx *ctx, const int32_t *gpack, int32_t nid, int3
     ctx->qm_valid = false;
     ctx->pm_valid = false;
     CK(epi::mma_encode_genotypes(&ctx->maps, ctx->d_hcodes, ctx->d_h3, nsnp, 32 * Wp));
-    CK(epi::popc_encode_planes(&ctx->pmaps, ctx->d_planes, nsnp, Wp));
     if (ctx->traits_nid != nid) ctx->ntraits = 0;  // traits no longer match
     ctx->nid = nid;
     ctx->nsnp = nsnp;
@@ -463,6 +466,7 @@ namespace {
 struct ScanRun {
     epi::ScanArgs args;
     int form;
+    int variant;  // the form's kernel variant (tile shape or ring depths)
     int64_t ntiles;
     std::vector<BlockDesc> desc;
 };
@@ -479,6 +483,7 @@ epi_status check_opts(epi_ctx *ctx, const epi_scan_opts *o)
     if (o->wait_limit_ms < 0) return set_err(ctx, EPI_E_INVALID, "wait_limit_ms must be >= 0");
     if (o->debug != 0 && o->debug != EPI_DEBUG_STALL) return set_err(ctx, EPI_E_INVALID, "bad debug flags");
     if (o->no_graph != 0 && o->no_graph != 1) return set_err(ctx, EPI_E_INVALID, "no_graph must be 0 or 1");
+    if (o->tile_config < 0) return set_err(ctx, EPI_E_INVALID, "tile_config must be >= 0");
     return EPI_OK;
 }
 
@@ -491,9 +496,11 @@ int pick_form(const epi_ctx *ctx, const epi_scan_opts *o)
 }
 
 // Builds the kernel arguments and tile schedule for `blocks` and uploads the schedule.
-epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const epi_scan_opts *o, ScanRun &r)
+epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const epi_scan_opts *o, ScanRun &r,
+                     int variant)
 {
     r.form = pick_form(ctx, o);
+    r.variant = variant;
     if (r.form == EPI_FORM_TENSOR && !epi::mma_available())
         return set_err(ctx, EPI_E_UNSUPPORTED, "tensor form not available in this build");
     if (r.form == EPI_FORM_TENSOR && ctx->Np > epi::mma_max_nid())
@@ -501,8 +508,11 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     if (r.form == EPI_FORM_POPC && ctx->nid > 65535)
         return set_err(ctx, EPI_E_UNSUPPORTED, "popcount form counts in 16 bits: at most 65535 individuals "
                        "(the reference's unsigned short counts, EpiOpenCL.c:68)");
-    const int TI = r.form == EPI_FORM_TENSOR ? epi::mma_tile_i() : epi::popc_tile_i();
-    const int TJ = r.form == EPI_FORM_TENSOR ? epi::mma_tile_j() : epi::popc_tile_j();
+    int TI = epi::mma_tile_i(), TJ = epi::mma_tile_j();
+    if (r.form == EPI_FORM_POPC) {
+        epi::popc_shape(variant, &TI, &TJ, nullptr);
+        CK(epi::popc_encode_planes(variant, &ctx->pmaps, ctx->d_planes, ctx->nsnp, ctx->Wp));
+    }
     r.desc.resize(nblocks);
     int64_t base = 0;
     for (int b = 0; b < nblocks; ++b) {
@@ -622,8 +632,8 @@ cudaError_t enqueue_scan(epi_ctx *ctx, const ScanRun &r, int grid, int nblocks, 
         e = cudaMemcpyAsync(ctx->d_blocks, ctx->h_blocks, nblocks * sizeof(BlockDesc), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev0, s, ev_flags);
     if (e == cudaSuccess && r.ntiles > 0)
-        e = r.form == EPI_FORM_TENSOR ? epi::mma_enqueue(r.args, ctx->maps, grid, s)
-                                      : epi::popc_enqueue(r.args, ctx->pmaps, grid, s);
+        e = r.form == EPI_FORM_TENSOR ? epi::mma_enqueue(r.variant, r.args, ctx->maps, grid, s)
+                                      : epi::popc_enqueue(r.variant, r.args, ctx->pmaps, grid, s);
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev1, s, ev_flags);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(ctx->h_state, ctx->d_counters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
@@ -651,10 +661,10 @@ epi_status launch_run(epi_ctx *ctx, ScanRun &r, int nblocks, bool use_graph)
         const int64_t units = r.ntiles * (int64_t)ctx->ntraits;
         if (r.form == EPI_FORM_TENSOR) {
             // one CTA pair per unit (tile x trait) up to every SM
-            CK(epi::mma_prepare(ctx->ntraits, (int)std::min<int64_t>(2 * units, ctx->sm_count), &grid));
+            CK(epi::mma_prepare(r.variant, ctx->ntraits, (int)std::min<int64_t>(2 * units, ctx->sm_count), &grid));
         } else {
             // one CTA per unit up to every SM
-            CK(epi::popc_prepare());
+            CK(epi::popc_prepare(r.variant));
             grid = (int)std::min<int64_t>(units, ctx->sm_count);
         }
     }
@@ -668,6 +678,7 @@ epi_status launch_run(epi_ctx *ctx, ScanRun &r, int nblocks, bool use_graph)
     std::vector<unsigned char> key;
     key_add(key, r.args);
     key_add(key, r.form);
+    key_add(key, r.variant);
     key_add(key, grid);
     key_add(key, ctx->ntraits);
     if (r.form == EPI_FORM_TENSOR) key_add(key, ctx->maps);
@@ -696,6 +707,99 @@ epi_status launch_run(epi_ctx *ctx, ScanRun &r, int nblocks, bool use_graph)
     return EPI_OK;
 }
 
+// ---- autotuner: the kernel variant per (device, form, padded individuals, traits) ----
+//
+// Every candidate of the form's table (tile shapes of the plain form, ring depths of the
+// tensor form) scans a sample block of the loaded genotypes and traits -- large enough for a
+// few waves of tiles over every SM -- once to warm up and once timed with CUDA events; the
+// fastest is kept for the process. The reference has one such knob, the chunk size of its
+// launches (src/main.c:115-130, src/EpiOpenCL.c:1353-1362), set by hand.
+struct TuneEntry {
+    int device, form, Np, ntraits, variant;
+    std::string how;
+};
+static std::mutex g_tune_mu;
+static std::vector<TuneEntry> g_tune;
+
+int form_variants(int form) { return form == EPI_FORM_TENSOR ? epi::mma_shapes() : epi::popc_shapes(); }
+
+std::string variant_desc(int form, int v)
+{
+    const char *d = nullptr;
+    int ti = 0, tj = 0;
+    if (form == EPI_FORM_TENSOR) epi::mma_shape(v, &d);
+    else epi::popc_shape(v, &ti, &tj, &d);
+    return std::string(form == EPI_FORM_TENSOR ? "tensor form, " : "plain form, ") + d;
+}
+
+epi_status pick_variant(epi_ctx *ctx, const epi_scan_opts *o, int form, int *v, std::string *how)
+{
+    const int nv = form_variants(form);
+    if (o->tile_config > 0) {
+        if (o->tile_config > nv)
+            return set_err(ctx, EPI_E_INVALID, "tile_config %d: this form has %d candidates", o->tile_config, nv);
+        *v = o->tile_config - 1;
+        *how = "requested";
+        return EPI_OK;
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        for (const TuneEntry &t : g_tune)
+            if (t.device == ctx->device && t.form == form && t.Np == ctx->Np && t.ntraits == ctx->ntraits) {
+                *v = t.variant;
+                *how = t.how;
+                return EPI_OK;
+            }
+    }
+    if (nv == 1) {
+        *v = 0;
+        *how = "only candidate";
+        return EPI_OK;
+    }
+    // sample: an off-diagonal s x s block (every pair valid) when the genome holds one, with
+    // enough tiles for about four waves over the SMs at this trait count
+    const int T = ctx->ntraits;
+    int s = (int)std::ceil(std::sqrt(4.0 * ctx->sm_count * 4096.0 / T));
+    s = std::max(256, std::min(s, 2048));
+    epi_block blk;
+    if (ctx->nsnp >= 2 * s) blk = {s, s, 0, s};
+    else blk = {0, ctx->nsnp, 0, ctx->nsnp};
+    if (ctx->hit_cap == 0) {
+        const int64_t initial = 1 << 20;
+        CK(cudaMalloc((void **)&ctx->d_hits, initial * sizeof(DevHit)));
+        ctx->hit_cap = initial;
+    }
+    epi_scan_opts o2 = *o;
+    o2.report_trait = 0;
+    std::vector<float> ms(nv, 0.0f);
+    for (int c = 0; c < nv; ++c) {
+        ScanRun r;
+        epi_status st = setup_run(ctx, &blk, 1, &o2, r, c);
+        if (st != EPI_OK) return st;
+        r.args.hits = ctx->d_hits;
+        r.args.cap = ctx->hit_cap;
+        for (int rep = 0; rep < 2; ++rep) {
+            st = launch_run(ctx, r, 1, false);
+            if (st != EPI_OK) return st;
+        }
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (ctx->h_state[2] != 0)
+            return set_err(ctx, EPI_E_TIMEOUT, "a bounded device wait gave up while tuning (site %llu)",
+                           ctx->h_state[3]);
+        CK(cudaEventElapsedTime(&ms[c], ctx->ev0, ctx->ev1));
+    }
+    const int best = (int)(std::min_element(ms.begin(), ms.end()) - ms.begin());
+    char buf[256];
+    int len = snprintf(buf, sizeof(buf), "autotuned on a %d x %d-SNP block:", blk.size1, blk.size2);
+    for (int c = 0; c < nv && len < (int)sizeof(buf); ++c)
+        len += snprintf(buf + len, sizeof(buf) - len, "%s %.3f ms", c ? " /" : "", ms[c]);
+    *v = best;
+    *how = buf;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune.push_back({ctx->device, form, ctx->Np, ctx->ntraits, best, *how});
+    return EPI_OK;
+}
+
 struct HitKey {
     int32_t trait, block, s, k, l, gx, gy;
     int64_t idx;
@@ -716,8 +820,13 @@ extern "C" epi_status epi_scan(epi_ctx *ctx, const epi_block *blocks, int32_t nb
     epi_status s = check_opts(ctx, opts);
     if (s != EPI_OK) return s;
     CK(cudaSetDevice(ctx->device));
+    const int form = pick_form(ctx, opts);
+    int variant = 0;
+    std::string how;
+    s = pick_variant(ctx, opts, form, &variant, &how);
+    if (s != EPI_OK) return s;
     ScanRun r;
-    s = setup_run(ctx, blocks, nblocks, opts, r);
+    s = setup_run(ctx, blocks, nblocks, opts, r, variant);
     if (s != EPI_OK) return s;
     if (ctx->hit_cap == 0) {
         const int64_t initial = 1 << 20;
@@ -748,6 +857,7 @@ extern "C" epi_status epi_scan(epi_ctx *ctx, const epi_block *blocks, int32_t nb
     float ms = 0.0f;
     CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     ctx->last_ms = ms;
+    ctx->last_config = variant_desc(form, variant) + " (" + how + ")";
     int64_t pairs = 0;
     for (int b = 0; b < nblocks; ++b) pairs += block_pairs(blocks[b]);
     ctx->last_pairs = pairs * ctx->ntraits;
@@ -820,8 +930,13 @@ extern "C" epi_status epi_scan_dump(epi_ctx *ctx, const epi_block *block, const 
     epi_status s = check_opts(ctx, &o);
     if (s != EPI_OK) return s;
     CK(cudaSetDevice(ctx->device));
+    const int form = pick_form(ctx, &o);
+    int variant = 0;
+    std::string how;
+    s = pick_variant(ctx, &o, form, &variant, &how);
+    if (s != EPI_OK) return s;
     ScanRun r;
-    s = setup_run(ctx, block, 1, &o, r);
+    s = setup_run(ctx, block, 1, &o, r, variant);
     if (s != EPI_OK) return s;
     const size_t np = (size_t)block->size1 * block->size2;
     int32_t *dc = nullptr, *dd1 = nullptr, *dd2 = nullptr;
@@ -865,6 +980,13 @@ extern "C" epi_status epi_scan_dump(epi_ctx *ctx, const epi_block *block, const 
     for (Out &x : outs)
         if (*x.dev) cudaFree(*x.dev);
     return st;
+}
+
+extern "C" epi_status epi_scan_config(const epi_ctx *ctx, char *desc, int32_t len)
+{
+    if (!ctx || !desc || len < 1) return EPI_E_INVALID;
+    snprintf(desc, (size_t)len, "%s", ctx->last_config.c_str());
+    return EPI_OK;
 }
 
 extern "C" epi_status epi_get_stream(const epi_ctx *ctx, void **stream)

@@ -117,9 +117,10 @@ struct MmaMaps {
     CUtensorMap hi, hj, dg;
 };
 
-// TMA descriptor of the plain form: the genotype plane words
+// TMA descriptors of the plain form: the genotype plane words, in boxes of the tile's i-SNPs
+// and of its j-SNPs
 struct PopcMaps {
-    CUtensorMap planes;
+    CUtensorMap planes_i, planes_j;
 };
 
 // float -> unsigned with the same order (for atomicMax over possibly negative F)

@@ -72,20 +72,6 @@ constexpr int N = 256;         // MMA width (pair MMAs take multiples of 32); co
 constexpr int NH = N / 2;      // B columns held by each CTA
 constexpr int M = 256;         // MMA height over the pair
 constexpr int KS = 128;        // individuals per pipeline stage
-// operand rings: A stages come by TMA from L2 / DRAM and need the deeper ring; B stages are
-// built from raw rows already in shared memory
-#ifndef EPI_MMA_ASTAGES
-#define EPI_MMA_ASTAGES 7
-#endif
-#ifndef EPI_MMA_BSTAGES
-#define EPI_MMA_BSTAGES 3
-#endif
-constexpr int ASTAGES = EPI_MMA_ASTAGES;
-constexpr int BSTAGES = EPI_MMA_BSTAGES;
-#ifndef EPI_MMA_RSTAGES
-#define EPI_MMA_RSTAGES 10
-#endif
-constexpr int RSTAGES = EPI_MMA_RSTAGES;  // raw ring (smem, TMA)
 constexpr int ND = 7;          // digit rows per trait: w, Y digits (3), E digits (3)
 constexpr int ROUNDS = (TJ + 2) / 3;  // j rounds of the epilogue (3 j-SNPs per round)
 constexpr uint32_t ACC_COL1 = N;
@@ -107,18 +93,25 @@ static_assert(B_STAGE % 1024 == 0 && A_STAGE % 1024 == 0 && N % 32 == 0 && N <= 
 static_assert(NCOL - NH == 7 * TJ && NH == 8 * TJ, "B split: CTA 0 types 0-7, CTA 1 types 8-14 + padding");
 static_assert(2 * N <= (int)TMEM_COLS && ROUNDS % 2 == 0, "TMEM layout / epilogue split");
 
-struct Smem {
-    uint8_t a[ASTAGES][A_STAGE];
-    uint8_t b[BSTAGES][B_STAGE];
-    uint8_t raw[RSTAGES][RAW_STAGE];
-    // bfull: B halves built (CTA 0: 4 local + 4 remote producer warps); afull: A stages landed
-    // (CTA 0: own TMA + CTA 1's forward; CTA 1: own TMA); aempty / bempty: the MMAs reading
-    // the slot are done (both CTAs)
-    uint64_t afull[ASTAGES], aempty[ASTAGES], bfull[BSTAGES], bempty[BSTAGES], raw_full[RSTAGES],
-        raw_empty[RSTAGES], acc_full[2], acc_empty[2], drain;
-    uint64_t stall;  // never arrived at: the wait of the debug_stall test hook
-    uint32_t tmem_base;
-    int abort;
+// Ring depths (a kernel variant, chosen by the autotuner): A stages come by TMA from L2 / DRAM
+// and need the deeper ring; B stages are built from raw rows already in shared memory; the raw
+// ring (j one-hot and digit rows, by TMA) lets the raw loader run ahead of the B producers.
+template <int AS, int BS, int RSx>
+struct Rings {
+    static constexpr int ASTAGES = AS, BSTAGES = BS, RSTAGES = RSx;
+    struct Smem {
+        uint8_t a[ASTAGES][A_STAGE];
+        uint8_t b[BSTAGES][B_STAGE];
+        uint8_t raw[RSTAGES][RAW_STAGE];
+        // bfull: B halves built (CTA 0: 4 local + 4 remote producer warps); afull: A stages landed
+        // (CTA 0: own TMA + CTA 1's forward; CTA 1: own TMA); aempty / bempty: the MMAs reading
+        // the slot are done (both CTAs)
+        uint64_t afull[ASTAGES], aempty[ASTAGES], bfull[BSTAGES], bempty[BSTAGES], raw_full[RSTAGES],
+            raw_empty[RSTAGES], acc_full[2], acc_empty[2], drain;
+        uint64_t stall;  // never arrived at: the wait of the debug_stall test hook
+        uint32_t tmem_base;
+        int abort;
+    };
 };
 
 // 16-byte chunk c of row r of a 128-byte-swizzled tile (1024-byte aligned base)
@@ -147,6 +140,7 @@ __device__ __forceinline__ Unit decode(const ScanArgs &a, long long u)
     return r;
 }
 
+template <class Smem>
 __device__ __forceinline__ void fail(const ScanArgs &a, Smem &sm, int where)
 {
     sm.abort = 1;
@@ -307,8 +301,11 @@ __device__ __forceinline__ void advance(uint32_t &slot, uint32_t &phase)
     }
 }
 
+template <class C>
 __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __grid_constant__ MmaMaps maps)
 {
+    constexpr int ASTAGES = C::ASTAGES, BSTAGES = C::BSTAGES, RSTAGES = C::RSTAGES;
+    using Smem = typename C::Smem;
     extern __shared__ uint8_t smem_raw[];
     // the operand stages need 1024-byte alignment (128-byte swizzle atoms); the offset is the
     // same in both CTAs of the pair, as the pair MMA and the remote arrivals require
@@ -819,11 +816,27 @@ int mma_min_nid() { return 256; }
 int mma_max_nid() { return 1 << 24; }  // digit sums stay within int32
 int mma_stage_individuals() { return mma::KS; }
 
-// Launch shape per (device, dynamic shared memory size): the attribute set and the number
-// of co-resident clusters, queried once (the occupancy query costs far more than a small
-// scan's host work).
+// The ring depths the autotuner chooses among (A, B, raw stages; each fills the SM's shared
+// memory to about 200 KB):
+//   0  7 / 3 / 10   1  6 / 4 / 8   2  8 / 3 / 6
+using Rings0 = mma::Rings<7, 3, 10>;
+using Rings1 = mma::Rings<6, 4, 8>;
+using Rings2 = mma::Rings<8, 3, 6>;
+constexpr int MMA_SHAPES = 3;
+
+int mma_shapes() { return MMA_SHAPES; }
+
+void mma_shape(int v, const char **desc)
+{
+    static const char *names[MMA_SHAPES] = {"rings A7/B3/R10", "rings A6/B4/R8", "rings A8/B3/R6"};
+    if (desc) *desc = names[v];
+}
+
+// Launch shape per (device, variant, dynamic shared memory size): the attribute set and the
+// number of co-resident clusters, queried once (the occupancy query costs far more than a
+// small scan's host work).
 struct MmaShape {
-    int device;
+    int device, variant;
     size_t smem;
     int clusters;
 };
@@ -831,6 +844,7 @@ struct MmaShape {
 static std::mutex g_shape_mu;
 static std::vector<MmaShape> g_shapes;
 
+template <class C>
 static cudaLaunchConfig_t mma_config(int ntraits, int grid, cudaStream_t stream, cudaLaunchAttribute *attr)
 {
     cudaLaunchConfig_t cfg = {};
@@ -842,52 +856,74 @@ static cudaLaunchConfig_t mma_config(int ntraits, int grid, cudaStream_t stream,
     cfg.blockDim = dim3(mma::NTHREADS, 1, 1);
     // more than half of the SM's shared memory: one CTA per SM, which owns all 512 TMEM
     // columns; the tail holds the per-CTA maxima
-    cfg.dynamicSmemBytes = sizeof(mma::Smem) + 1024 + smax_bytes(ntraits);
+    cfg.dynamicSmemBytes = sizeof(typename C::Smem) + 1024 + smax_bytes(ntraits);
     cfg.stream = stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cfg;
 }
 
-// The launch shape of a scan, resolved before any stream capture: the kernel's shared-memory
-// attribute and the number of co-resident clusters (queried once per device and size), then
-// whole clusters of two -- at least one, never more than can be resident at once.
-cudaError_t mma_prepare(int ntraits, int grid_request, int *grid)
+template <class C>
+static cudaError_t prepare(int v, int ntraits, int grid_request, int *grid)
 {
-    static_assert(sizeof(mma::Smem) + 1024 > 116 * 1024, "one CTA per SM");
+    static_assert(sizeof(typename C::Smem) + 1024 > 116 * 1024, "one CTA per SM");
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return e;
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = mma_config(ntraits, std::max(2, (grid_request + 1) & ~1), nullptr, attr);
+    cudaLaunchConfig_t cfg = mma_config<C>(ntraits, std::max(2, (grid_request + 1) & ~1), nullptr, attr);
     int clusters = 0;
     {
         std::lock_guard<std::mutex> lock(g_shape_mu);
         for (const MmaShape &sh : g_shapes)
-            if (sh.device == device && sh.smem == cfg.dynamicSmemBytes) clusters = sh.clusters;
+            if (sh.device == device && sh.variant == v && sh.smem == cfg.dynamicSmemBytes) clusters = sh.clusters;
         if (clusters == 0) {
             // the attribute admits the largest size any trait count asks for
-            e = cudaFuncSetAttribute(mma::k_scan_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(sizeof(mma::Smem) + 1024 + smax_bytes(SMAX_TRAITS)));
+            e = cudaFuncSetAttribute(mma::k_scan_mma<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(sizeof(typename C::Smem) + 1024 + smax_bytes(SMAX_TRAITS)));
             if (e != cudaSuccess) return e;
-            e = cudaOccupancyMaxActiveClusters(&clusters, mma::k_scan_mma, &cfg);
+            e = cudaOccupancyMaxActiveClusters(&clusters, mma::k_scan_mma<C>, &cfg);
             if (e != cudaSuccess) return e;
             if (clusters < 1) return cudaErrorInvalidConfiguration;
-            g_shapes.push_back({device, cfg.dynamicSmemBytes, clusters});
+            g_shapes.push_back({device, v, cfg.dynamicSmemBytes, clusters});
         }
     }
     *grid = std::min((int)cfg.gridDim.x, 2 * clusters);
     return cudaSuccess;
 }
 
-// The launch itself (a stream operation only, so it can be captured into a CUDA graph).
-cudaError_t mma_enqueue(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream)
+template <class C>
+static cudaError_t enqueue(const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream)
 {
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = mma_config(a.ntraits, grid, stream, attr);
-    cudaError_t e = cudaLaunchKernelEx(&cfg, mma::k_scan_mma, a, maps);
+    cudaLaunchConfig_t cfg = mma_config<C>(a.ntraits, grid, stream, attr);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, mma::k_scan_mma<C>, a, maps);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
+}
+
+// The launch shape of a scan with variant v, resolved before any stream capture: the kernel's
+// shared-memory attribute and the number of co-resident clusters, then whole clusters of two --
+// at least one, never more than can be resident at once.
+cudaError_t mma_prepare(int v, int ntraits, int grid_request, int *grid)
+{
+    switch (v) {
+    case 0: return prepare<Rings0>(v, ntraits, grid_request, grid);
+    case 1: return prepare<Rings1>(v, ntraits, grid_request, grid);
+    case 2: return prepare<Rings2>(v, ntraits, grid_request, grid);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// The launch itself (a stream operation only, so it can be captured into a CUDA graph).
+cudaError_t mma_enqueue(int v, const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream)
+{
+    switch (v) {
+    case 0: return enqueue<Rings0>(a, maps, grid, stream);
+    case 1: return enqueue<Rings1>(a, maps, grid, stream);
+    case 2: return enqueue<Rings2>(a, maps, grid, stream);
+    }
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace epi

@@ -2,9 +2,10 @@
 // (src/EpiOpenCL.c:110-228: unpack two SNPs, count the 3x3 genotype cells, add the
 // phenotype into its cell) redone for the B200's CUDA cores.
 //
-// Persistent kernel, one 512-thread CTA per SM, pulling (64 x 64 SNP-pair tile, trait) units
-// from a queue over the tile schedule of the chromosome blocks. The genotype bit-plane words of
-// the tile's 64 i-SNPs and 64 j-SNPs (planes of g==0, g==1, g==2, g!=3 per 32 individuals)
+// Persistent kernel, one 512-thread CTA per SM, pulling (SNP-pair tile, trait) units from a
+// queue over the tile schedule of the chromosome blocks (tile shapes: the table at the end of
+// this file, chosen by the autotuner). The genotype bit-plane words of the tile's i-SNPs and
+// j-SNPs (planes of g==0, g==1, g==2, g!=3 per 32 individuals)
 // arrive by TMA, 64 individuals per stage, in a three-stage ring. Each SNP's two genotypes
 // other than its most frequent one are its dense genotypes A and B. Per stage:
 //   * expansion (all threads, double-buffered): for each i-SNP, U_A = [g_i==A]*y and
@@ -35,33 +36,37 @@
 namespace epi {
 namespace popc {
 
-constexpr int WI = 8;              // warps along i
-constexpr int WJ = 2;              // warps along j
-constexpr int PI = 8;              // i-SNPs per warp = pairs per thread
-constexpr int TI = WI * PI;        // 64 i-SNPs per tile
-constexpr int TJ = WJ * 32;        // 64 j-SNPs per tile
-constexpr int NT = WI * WJ * 32;   // 512 threads
-constexpr int KW = 2;              // 32-individual words per stage
-constexpr int KI = 32 * KW;        // 64 individuals per stage
-constexpr int KP = KI / 2;         // individual pairs per stage
-constexpr int RS = 3;              // TMA ring depth
-constexpr uint32_t STAGE_BYTES = (TI + TJ) * KW * 16;  // transaction bytes per stage
-static_assert(TI == TJ, "one tensor map box serves both sides");
+// A tile shape: WI x WJ warps, each warp PI i-SNPs x 32 j-SNPs (PI pairs per thread); the
+// tile is TI = WI * PI i-SNPs by TJ = 32 * WJ j-SNPs. The autotuner picks one per device and
+// workload from the table at the end of this file.
+template <int WI_, int WJ_, int PI_>
+struct Shape {
+    static constexpr int WI = WI_, WJ = WJ_, PI = PI_;
+    static constexpr int TI = WI * PI;        // i-SNPs per tile
+    static constexpr int TJ = WJ * 32;        // j-SNPs per tile
+    static constexpr int NT = WI * WJ * 32;   // threads
+    static constexpr int KW = 2;              // 32-individual words per stage
+    static constexpr int KI = 32 * KW;        // individuals per stage
+    static constexpr int KP = KI / 2;         // individual pairs per stage
+    static constexpr int RS = 3;              // TMA ring depth
+    static constexpr uint32_t STAGE_BYTES = (TI + TJ) * KW * 16;  // transaction bytes per stage
+    static_assert(TI * KW <= NT - KI / 4 && TI <= 256 && TJ <= 256 && TI + TJ <= NT, "expansion roles");
 
-struct Smem {
-    uint4 raw_i[RS][TI][KW];  // TMA: plane words of the i-tile (row = SNP)
-    uint4 raw_j[RS][TJ][KW];  // TMA: plane words of the j-tile
-    float4 u[2][KP][TI];      // (U_A(k), U_A(k+1), U_B(k), U_B(k+1)) of each i-SNP
-    uint4 pm[2][KW][TI];      // (P_A & W, P_B & W, missing & W, W) of each i-SNP
-    float y[2][KI];           // the stage's trait values (0 where invalid)
-    float4 sps[PI][NT];       // per pair: sums over individuals missing at i by g_j: S_30..S_32, QMM
-    uint2 spn[PI][NT];        // and counts: n_30 | n_31 << 16, n_32
-    float2 spj[PI][NT];       // per pair: sums over individuals missing at j by g_i: S_{Ai,3}, S_{Bi,3}
-    uint64_t full[RS];
-    uint8_t maj[TI];          // most frequent genotype of each i-SNP
-    uint8_t majj[TJ];         // and of each j-SNP
-    long long unit;
-    int never;                // always 0: the abort flag of the bounded waits
+    struct Smem {
+        uint4 raw_i[RS][TI][KW];  // TMA: plane words of the i-tile (row = SNP)
+        uint4 raw_j[RS][TJ][KW];  // TMA: plane words of the j-tile
+        float4 u[2][KP][TI];      // (U_A(k), U_A(k+1), U_B(k), U_B(k+1)) of each i-SNP
+        uint4 pm[2][KW][TI];      // (P_A & W, P_B & W, missing & W, W) of each i-SNP
+        float y[2][KI];           // the stage's trait values (0 where invalid)
+        float4 sps[PI][NT];       // per pair: sums over individuals missing at i by g_j: S_30..S_32, QMM
+        uint2 spn[PI][NT];        // and counts: n_30 | n_31 << 16, n_32
+        float2 spj[PI][NT];       // per pair: sums over individuals missing at j by g_i: S_{Ai,3}, S_{Bi,3}
+        uint64_t full[RS];
+        uint8_t maj[TI];          // most frequent genotype of each i-SNP
+        uint8_t majj[TJ];         // and of each j-SNP
+        long long unit;
+        int never;                // always 0: the abort flag of the bounded waits
+    };
 };
 
 // One pair's accumulators and the per-SNP values its statistics need, passed out of line.
@@ -130,8 +135,12 @@ __device__ __noinline__ PairStat eval_pair(const ScanArgs &a, const PairIn p)
 
 __device__ __forceinline__ bool bit(uint32_t w, int t) { return (w >> t) & 1u; }
 
-__global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a, const __grid_constant__ PopcMaps maps)
+template <class Sh>
+__global__ void __launch_bounds__(Sh::NT, 1) k_scan_popc(ScanArgs a, const __grid_constant__ PopcMaps maps)
 {
+    constexpr int WI = Sh::WI, PI = Sh::PI, TI = Sh::TI, TJ = Sh::TJ, NT = Sh::NT, KW = Sh::KW, KI = Sh::KI;
+    constexpr int RS = Sh::RS;
+    using Smem = typename Sh::Smem;
     extern __shared__ uint8_t smem_raw[];
     // TMA destinations: 1024-byte aligned
     const uint32_t raw_s = tc::smem_u32(smem_raw);
@@ -196,19 +205,19 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a, const __grid_co
         }
         auto issue = [&](int st) {  // thread 0: the TMA loads of stage st
             const int r = st % RS;
-            tc::mbar_arrive_expect_tx(&sm.full[r], STAGE_BYTES);
-            tc::tma_load_2d(&sm.raw_i[r][0][0], &maps.planes, 4 * KW * st, bd.start1 + i0, &sm.full[r]);
-            tc::tma_load_2d(&sm.raw_j[r][0][0], &maps.planes, 4 * KW * st, bd.start2 + j0, &sm.full[r]);
+            tc::mbar_arrive_expect_tx(&sm.full[r], Sh::STAGE_BYTES);
+            tc::tma_load_2d(&sm.raw_i[r][0][0], &maps.planes_i, 4 * KW * st, bd.start1 + i0, &sm.full[r]);
+            tc::tma_load_2d(&sm.raw_j[r][0][0], &maps.planes_j, 4 * KW * st, bd.start2 + j0, &sm.full[r]);
         };
         if (tid == 0)
             for (int st = 0; st < min(RS, nst); ++st) issue(st);
         __syncthreads();  // maj
 
-        // expansion of stage st into buffer b: thread -> (i-SNP, 8 individuals)
+        // expansion of stage st into buffer b: work item -> (i-SNP, 8 individuals)
         auto expand = [&](int st, int b) {
             const int r = st % RS;
-            {
-                const int i = tid >> 3, part = tid & 7, w = part >> 2, k8 = 8 * (part & 3);
+            for (int it = tid; it < 8 * TI; it += NT) {
+                const int i = it >> 3, part = it & 7, w = part >> 2, k8 = 8 * (part & 3);
                 const uint4 P = sm.raw_i[r][i][w];
                 const int mj = sm.maj[i];
                 const uint32_t PA = mj == 0 ? P.y : P.x, PB = mj == 2 ? P.y : P.z;
@@ -230,8 +239,8 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a, const __grid_co
                 const uint32_t W = __ldg(wt + KW * st + w);
                 const uint32_t PA = mj == 0 ? P.y : P.x, PB = mj == 2 ? P.y : P.z;
                 sm.pm[b][w][i] = make_uint4(PA & W, PB & W, ~P.w & W, W);
-            } else if (tid < TI * KW + KI / 4) {
-                const int q = tid - TI * KW;
+            } else if (tid >= NT - KI / 4) {
+                const int q = tid - (NT - KI / 4);
                 reinterpret_cast<float4 *>(sm.y[b])[q] = __ldg(reinterpret_cast<const float4 *>(yt + KI * st) + q);
             }
         };
@@ -369,13 +378,33 @@ __global__ void __launch_bounds__(NT, 1) k_scan_popc(ScanArgs a, const __grid_co
 
 }  // namespace popc
 
-// Tile shape of this form (used by the host to build the tile schedule).
-int popc_tile_i() { return popc::TI; }
-int popc_tile_j() { return popc::TJ; }
+// The tile shapes the autotuner chooses among:
+//   0  64 x 64 tile, 8 pairs per thread (8 x 2 warps): fewest shared-memory loads per add
+//   1  64 x 32 tile, 4 pairs per thread (16 x 1 warps): fewest registers, most warps per i-SNP
+//   2  32 x 128 tile, 8 pairs per thread (4 x 4 warps): the i-side expansion shared by more lanes
+using Shape0 = popc::Shape<8, 2, 8>;
+using Shape1 = popc::Shape<16, 1, 4>;
+using Shape2 = popc::Shape<4, 4, 8>;
+constexpr int POPC_SHAPES = 3;
 
-// The plane words [nsnp][Wp] (uint4) as a 2-D uint32 tensor [nsnp][4 Wp], one box = the words
-// of one stage (KW x 4 uint32 = 32 bytes) of a 64-SNP tile; rows past the last SNP read as 0.
-cudaError_t popc_encode_planes(PopcMaps *maps, const uint4 *planes, int nsnp, int Wp)
+int popc_shapes() { return POPC_SHAPES; }
+
+// Tile size (i x j SNPs) and a description of shape v.
+void popc_shape(int v, int *ti, int *tj, const char **desc)
+{
+    static const char *names[POPC_SHAPES] = {"64x64 tile, 8 pairs/thread, 8x2 warps",
+                                             "64x32 tile, 4 pairs/thread, 16x1 warps",
+                                             "32x128 tile, 8 pairs/thread, 4x4 warps"};
+    const int tis[POPC_SHAPES] = {Shape0::TI, Shape1::TI, Shape2::TI};
+    const int tjs[POPC_SHAPES] = {Shape0::TJ, Shape1::TJ, Shape2::TJ};
+    *ti = tis[v];
+    *tj = tjs[v];
+    if (desc) *desc = names[v];
+}
+
+// The plane words [nsnp][Wp] (uint4) as a 2-D uint32 tensor [nsnp][4 Wp]; one box = the words
+// of one stage (KW x 4 uint32 = 32 bytes) of `rows` SNPs; rows past the last SNP read as 0.
+static cudaError_t encode_planes(CUtensorMap *m, const uint4 *planes, int nsnp, int Wp, int rows)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
@@ -387,29 +416,64 @@ cudaError_t popc_encode_planes(PopcMaps *maps, const uint4 *planes, int nsnp, in
     }
     const cuuint64_t dims[2] = {4 * (cuuint64_t)Wp, (cuuint64_t)nsnp};
     const cuuint64_t strides[1] = {16 * (cuuint64_t)Wp};
-    const cuuint32_t box[2] = {4 * popc::KW, popc::TI};
+    const cuuint32_t box[2] = {4 * Shape0::KW, (cuuint32_t)rows};
     const cuuint32_t es[2] = {1, 1};
-    CUresult r = encode(&maps->planes, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<uint4 *>(planes), dims, strides,
-                        box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<uint4 *>(planes), dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-static size_t popc_smem(int ntraits) { return sizeof(popc::Smem) + 1024 + smax_bytes(ntraits); }
-
-// Before any stream capture: the kernel's shared-memory attribute (the largest size any trait
-// count asks for).
-cudaError_t popc_prepare()
+cudaError_t popc_encode_planes(int v, PopcMaps *maps, const uint4 *planes, int nsnp, int Wp)
 {
-    return cudaFuncSetAttribute(popc::k_scan_popc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)popc_smem(SMAX_TRAITS));
+    int ti = 0, tj = 0;
+    popc_shape(v, &ti, &tj, nullptr);
+    cudaError_t e = encode_planes(&maps->planes_i, planes, nsnp, Wp, ti);
+    if (e == cudaSuccess) e = encode_planes(&maps->planes_j, planes, nsnp, Wp, tj);
+    return e;
+}
+
+template <class C>
+static size_t shape_smem(int ntraits)
+{
+    return sizeof(typename C::Smem) + 1024 + smax_bytes(ntraits);
+}
+
+template <class C>
+static cudaError_t prepare(void)
+{
+    return cudaFuncSetAttribute(popc::k_scan_popc<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)shape_smem<C>(SMAX_TRAITS));
+}
+
+template <class C>
+static cudaError_t enqueue(const ScanArgs &a, const PopcMaps &maps, int grid, cudaStream_t stream)
+{
+    popc::k_scan_popc<C><<<grid, C::NT, shape_smem<C>(a.ntraits), stream>>>(a, maps);
+    return cudaGetLastError();
+}
+
+// Before any stream capture: the shape's kernel attribute (the largest shared-memory size any
+// trait count asks for).
+cudaError_t popc_prepare(int v)
+{
+    switch (v) {
+    case 0: return prepare<Shape0>();
+    case 1: return prepare<Shape1>();
+    case 2: return prepare<Shape2>();
+    }
+    return cudaErrorInvalidValue;
 }
 
 // The launch itself (a stream operation only, so it can be captured into a CUDA graph).
-cudaError_t popc_enqueue(const ScanArgs &a, const PopcMaps &maps, int grid, cudaStream_t stream)
+cudaError_t popc_enqueue(int v, const ScanArgs &a, const PopcMaps &maps, int grid, cudaStream_t stream)
 {
-    popc::k_scan_popc<<<grid, popc::NT, popc_smem(a.ntraits), stream>>>(a, maps);
-    return cudaGetLastError();
+    switch (v) {
+    case 0: return enqueue<Shape0>(a, maps, grid, stream);
+    case 1: return enqueue<Shape1>(a, maps, grid, stream);
+    case 2: return enqueue<Shape2>(a, maps, grid, stream);
+    }
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace epi

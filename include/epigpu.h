@@ -77,7 +77,11 @@ typedef struct epi_scan_opts {
     int32_t no_graph;      /* 0: the scan's device work is captured as a CUDA graph and a repeat of
                             * the same scan shape (kernel arguments, blocks) replays it with one
                             * launch; 1: every operation is launched directly */
-    int32_t reserved[6];   /* set to 0 */
+    int32_t tile_config;   /* 0: the kernel variant (plain form: tile shape; tensor form: ring
+                            * depths) is chosen by the autotuner, which times every candidate
+                            * on a sample block once per device, form, individual count and
+                            * trait count; k >= 1: candidate k (epi_scan_config names it) */
+    int32_t reserved[5];   /* set to 0 */
 } epi_scan_opts;
 
 #define EPI_DEBUG_STALL 1
@@ -154,6 +158,11 @@ epi_status epi_scan_dump(epi_ctx *ctx, const epi_block *block, const epi_scan_op
  * form ran (EPI_FORM_POPC or EPI_FORM_TENSOR). Any output may be NULL. */
 epi_status epi_last_timing(const epi_ctx *ctx, double *kernel_ms, int64_t *pairs,
                            int32_t *launches, int32_t *form);
+
+/* The form and kernel variant the last epi_scan ran, and how the variant was chosen (the
+ * autotuner's timings of every candidate, or "requested"), as text. No counterpart in the
+ * reference, whose only tuning knob is the chunk size of its launches (src/main.c:115-130). */
+epi_status epi_scan_config(const epi_ctx *ctx, char *desc, int32_t len);
 
 /* The context's CUDA stream (a cudaStream_t, returned as an opaque pointer): every copy
  * and kernel of the context runs on it, so a caller can order or time its own work
