@@ -85,20 +85,29 @@ constexpr uint32_t A_BYTES = 4 * A_BOX * KS;  // transaction bytes per A stage (
 constexpr int RAW_J = 0, RAW_D = TJ * KS;
 constexpr int RAW_STAGE = 4 * 1024;
 constexpr uint32_t RAW_BYTES = (TJ + ND) * KS;
-constexpr int NWARPS = 15;
-constexpr int NTHREADS = NWARPS * 32;
+
 constexpr uint32_t IDESC = tc::idesc_i8(M, N);
 static_assert(RAW_D % 1024 == 0 && RAW_D + ND * KS <= RAW_STAGE, "raw layout");
 static_assert(B_STAGE % 1024 == 0 && A_STAGE % 1024 == 0 && N % 32 == 0 && N <= 256 && NCOL <= N, "operand tiles");
 static_assert(NCOL - NH == 7 * TJ && NH == 8 * TJ, "B split: CTA 0 types 0-7, CTA 1 types 8-14 + padding");
-static_assert(2 * N <= (int)TMEM_COLS && ROUNDS % 2 == 0, "TMEM layout / epilogue split");
+static_assert(2 * N <= (int)TMEM_COLS && ROUNDS % 6 == 0, "TMEM layout / epilogue split");
 
 // Ring depths (a kernel variant, chosen by the autotuner): A stages come by TMA from L2 / DRAM
 // and need the deeper ring; B stages are built from raw rows already in shared memory; the raw
 // ring (j one-hot and digit rows, by TMA) lets the raw loader run ahead of the B producers.
-template <int AS, int BS, int RSx>
+//
+// EPW epilogue warps per TMEM lane quarter: 2 (15 warps: epilogue 0-3 and 8-11) or 3 (20 warps:
+// epilogue also 16-19, warp 15 idle). With 3, the 640 threads launch with 96 registers each
+// and the warpgroups rebalance (setmaxnreg): the three epilogue warpgroups to 128, the B
+// producers to 56, the loaders and MMA issuer to 40 -- 3 x 128 x 128 + 128 x 56 + 128 x 40
+// = 61,440 = 640 x 96, the launch's pool.
+template <int AS, int BS, int RSx, int EPW_ = 2>
 struct Rings {
-    static constexpr int ASTAGES = AS, BSTAGES = BS, RSTAGES = RSx;
+    static constexpr int ASTAGES = AS, BSTAGES = BS, RSTAGES = RSx, EPW = EPW_;
+    static constexpr int NWARPS = EPW == 2 ? 15 : 20;
+    static constexpr int NTHREADS = NWARPS * 32;
+    static_assert(EPW == 2 || EPW == 3, "epilogue warps per lane quarter");
+    static_assert(EPW == 2 || 3 * 128 * 128 + 128 * 56 + 128 * 40 == NTHREADS * 96, "register split");
     struct Smem {
         uint8_t a[ASTAGES][A_STAGE];
         uint8_t b[BSTAGES][B_STAGE];
@@ -302,9 +311,9 @@ __device__ __forceinline__ void advance(uint32_t &slot, uint32_t &phase)
 }
 
 template <class C>
-__global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __grid_constant__ MmaMaps maps)
+__global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const __grid_constant__ MmaMaps maps)
 {
-    constexpr int ASTAGES = C::ASTAGES, BSTAGES = C::BSTAGES, RSTAGES = C::RSTAGES;
+    constexpr int ASTAGES = C::ASTAGES, BSTAGES = C::BSTAGES, RSTAGES = C::RSTAGES, EPW = C::EPW;
     using Smem = typename C::Smem;
     extern __shared__ uint8_t smem_raw[];
     // the operand stages need 1024-byte alignment (128-byte swizzle atoms); the offset is the
@@ -351,7 +360,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
         }
         for (int b = 0; b < 2; ++b) {
             tc::mbar_init(&sm.acc_full[b], 1);
-            tc::mbar_init(&sm.acc_empty[b], 16);
+            tc::mbar_init(&sm.acc_empty[b], 8 * EPW);  // every epilogue warp of both CTAs
         }
         tc::mbar_init(&sm.drain, 1);
         tc::mbar_init(&sm.stall, 1);
@@ -365,6 +374,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
     const uint32_t tmem = sm.tmem_base;
     volatile int *abort = &sm.abort;
 
+    // epilogue warps: 0-3, 8-11 (and 16-19 with three per lane quarter)
+    const bool epi_warp = warp < 4 || (warp >= 8 && warp < 12) || warp >= 16;
+    if constexpr (EPW == 3) {
+        if (epi_warp) tc::setmaxnreg_inc<128>();
+        else if (warp >= 4 && warp < 8) tc::setmaxnreg_dec<56>();
+        else tc::setmaxnreg_dec<40>();
+    }
     if (warp >= 4 && warp < 8) {
         // ---------------- B producers: thread -> (j-SNP, 16-individual chunk) ----------------
         const int t = threadIdx.x - 128, jj = t >> 3, c = t & 7;
@@ -443,9 +459,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 advance<RSTAGES>(rs, rph);
             }
         }
-    } else if (warp < 12) {
+    } else if (epi_warp) {
         // ---------------- epilogue: warps 0-3 rounds 0-2, warps 8-11 rounds 3-5 ----------------
-        const int e = warp & 3, rho0 = warp < 4 ? 0 : ROUNDS / 2;
+        constexpr int RPW = ROUNDS / EPW;  // j rounds per epilogue warp
+        const int e = warp & 3, rho0 = (warp < 4 ? 0 : (warp < 12 ? 1 : 2)) * RPW;
         const int ii = 10 * e + lane / 3, ga = lane % 3, tbase = (lane / 3) * 3;
         const bool rowok = lane < 30;
         const uint32_t tl = tmem + ((uint32_t)(32 * e) << 16);
@@ -479,7 +496,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
             const unsigned int m2 = reinterpret_cast<volatile unsigned int *>(mxf2)[t];
             float fmx_f = m1 ? ord2f(m1) : -INFINITY, f2mx_f = m2 ? ord2f(m2) : -INFINITY;
 #pragma unroll 1
-            for (int rho = rho0; rho < rho0 + ROUNDS / 2; ++rho) {
+            for (int rho = rho0; rho < rho0 + RPW; ++rho) {
                 const int jb = 3 * rho;
                 const int jl = jb + ga;
                 const int dj = un.j0 + jl;
@@ -690,7 +707,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 if (!tc::mbar_wait(&sm.raw_full[slot], par, &no_abort, a.wait_ns)) fail(a, sm, 11);
             }
         }
-    } else if (lane == 0 && rank == 1) {
+    } else if (warp == 12 && lane == 0 && rank == 1) {
         // ---------------- A forwarder (CTA 1, warp 12) ----------------
         // each of this CTA's A stages, once landed, counts as one arrival on CTA 0's afull
         uint32_t as = 0, aph = 0;
@@ -708,7 +725,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_scan_mma(ScanArgs a, const __gr
                 advance<ASTAGES>(as, aph);
             }
         }
-    } else if (lane == 0) {
+    } else if (warp == 12 && lane == 0) {
         // ---------------- MMA issuer (CTA 0, warp 12) ----------------
         uint32_t as = 0, aph = 0, bs = 0, bph = 0, accph[2] = {0u, 0u};
         int buf = 0;
@@ -816,19 +833,22 @@ int mma_min_nid() { return 256; }
 int mma_max_nid() { return 1 << 24; }  // digit sums stay within int32
 int mma_stage_individuals() { return mma::KS; }
 
-// The ring depths the autotuner chooses among (A, B, raw stages; each fills the SM's shared
-// memory to about 200 KB):
-//   0  7 / 3 / 10   1  6 / 4 / 8   2  8 / 3 / 6
+// The variants the autotuner chooses among -- ring depths (A, B, raw stages; each fills the
+// SM's shared memory to about 200 KB) and epilogue warps per TMEM lane quarter:
+//   0  7 / 3 / 10, 2 epilogue warps   1  6 / 4 / 8, 2   2  8 / 3 / 6, 2   3  7 / 3 / 10, 3
 using Rings0 = mma::Rings<7, 3, 10>;
 using Rings1 = mma::Rings<6, 4, 8>;
 using Rings2 = mma::Rings<8, 3, 6>;
-constexpr int MMA_SHAPES = 3;
+using Rings3 = mma::Rings<7, 3, 10, 3>;
+constexpr int MMA_SHAPES = 4;
 
 int mma_shapes() { return MMA_SHAPES; }
 
 void mma_shape(int v, const char **desc)
 {
-    static const char *names[MMA_SHAPES] = {"rings A7/B3/R10", "rings A6/B4/R8", "rings A8/B3/R6"};
+    static const char *names[MMA_SHAPES] = {"rings A7/B3/R10, 8 epilogue warps", "rings A6/B4/R8, 8 epilogue warps",
+                                            "rings A8/B3/R6, 8 epilogue warps",
+                                            "rings A7/B3/R10, 12 epilogue warps (setmaxnreg)"};
     if (desc) *desc = names[v];
 }
 
@@ -853,7 +873,7 @@ static cudaLaunchConfig_t mma_config(int ntraits, int grid, cudaStream_t stream,
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.gridDim = dim3((unsigned)grid, 1, 1);
-    cfg.blockDim = dim3(mma::NTHREADS, 1, 1);
+    cfg.blockDim = dim3(C::NTHREADS, 1, 1);
     // more than half of the SM's shared memory: one CTA per SM, which owns all 512 TMEM
     // columns; the tail holds the per-CTA maxima
     cfg.dynamicSmemBytes = sizeof(typename C::Smem) + 1024 + smax_bytes(ntraits);
@@ -911,6 +931,7 @@ cudaError_t mma_prepare(int v, int ntraits, int grid_request, int *grid)
     case 0: return prepare<Rings0>(v, ntraits, grid_request, grid);
     case 1: return prepare<Rings1>(v, ntraits, grid_request, grid);
     case 2: return prepare<Rings2>(v, ntraits, grid_request, grid);
+    case 3: return prepare<Rings3>(v, ntraits, grid_request, grid);
     }
     return cudaErrorInvalidValue;
 }
@@ -922,6 +943,7 @@ cudaError_t mma_enqueue(int v, const ScanArgs &a, const MmaMaps &maps, int grid,
     case 0: return enqueue<Rings0>(a, maps, grid, stream);
     case 1: return enqueue<Rings1>(a, maps, grid, stream);
     case 2: return enqueue<Rings2>(a, maps, grid, stream);
+    case 3: return enqueue<Rings3>(a, maps, grid, stream);
     }
     return cudaErrorInvalidValue;
 }

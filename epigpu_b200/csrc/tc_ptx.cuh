@@ -90,6 +90,24 @@ __device__ __forceinline__ void fence_barrier_init()
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Per-warpgroup register budgets (every thread of the 4 warps of a warpgroup executes it):
+// raise to / lower to REGS registers per thread. A raise waits until enough registers are free
+// in the pool the CTA was launched with, so the budgets of all warpgroups must sum to at most
+// that pool (threads x registers per thread at launch).
+template <int REGS>
+__device__ __forceinline__ void setmaxnreg_inc()
+{
+    static_assert(REGS % 8 == 0 && REGS >= 24 && REGS <= 256, "register count");
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REGS));
+}
+
+template <int REGS>
+__device__ __forceinline__ void setmaxnreg_dec()
+{
+    static_assert(REGS % 8 == 0 && REGS >= 24 && REGS <= 256, "register count");
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REGS));
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 

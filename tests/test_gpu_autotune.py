@@ -1,7 +1,8 @@
 """Kernel variants and the autotuner.
 
 Each form has a table of kernel variants (plain form: tile shapes -- 64 x 64 with 8 pairs per
-thread, 64 x 32 with 4, 32 x 128 with 8; tensor form: operand ring depths). Every variant must
+thread, 64 x 32 with 4, 32 x 128 with 8; tensor form: operand ring depths, and 8 or 12
+epilogue warps). Every variant must
 give the oracle's results: counts and df exact, F within the parity bar, the same hits in the
 same order (several uneven chromosome blocks, several traits with their own masks). The
 autotuner times every candidate once per device, form, individual count and trait count and
@@ -17,11 +18,12 @@ pytestmark = pytest.mark.gpu
 
 F_TOL = 1e-5
 TOL_SET = 1e-4
-N_CANDIDATES = 3
+N_CANDIDATES = {capi.FORM_POPC: 3, capi.FORM_TENSOR: 4}
+VARIANTS = [(f, c) for f in (capi.FORM_POPC, capi.FORM_TENSOR) for c in range(1, N_CANDIDATES[f] + 1)]
 
 
-@pytest.mark.parametrize("form", [capi.FORM_POPC, capi.FORM_TENSOR], ids=["popc", "tensor"])
-@pytest.mark.parametrize("cand", range(1, N_CANDIDATES + 1))
+@pytest.mark.parametrize("form,cand", VARIANTS,
+                         ids=["%s%d" % ("popc" if f == capi.FORM_POPC else "tensor", c) for f, c in VARIANTS])
 def test_every_variant_matches_oracle(gpu_ctx, form, cand):
     nid, sizes = 611, [150, 97, 201]
     codes = synth.genotype_codes(nid, sum(sizes), seed=401)
@@ -71,12 +73,13 @@ def test_autotuner_choice_is_reported_and_kept(gpu_ctx, form):
     opts = capi.default_opts(test="f", t1=t1, form=form)
     first, n1, _ = gpu_ctx.scan([(0, nsnp, 0, nsnp)], opts)
     cfg = gpu_ctx.scan_config()
-    assert "autotuned" in cfg and cfg.count(" ms") == N_CANDIDATES, cfg
+    nc = N_CANDIDATES[form]
+    assert "autotuned" in cfg and cfg.count(" ms") == nc, cfg
     again, n2, _ = gpu_ctx.scan([(0, nsnp, 0, nsnp)], opts)
     assert gpu_ctx.scan_config() == cfg  # kept, not tuned again
     assert n1 == n2 and np.array_equal(first, again)
     # the chosen candidate, requested by number, gives the same hits
-    names = {k: None for k in range(1, N_CANDIDATES + 1)}
+    names = {k: None for k in range(1, nc + 1)}
     for k in names:
         gpu_ctx.scan([(0, 10, 0, 10)], capi.default_opts(test="f", t1=t1, form=form, tile_config=k))
         names[k] = gpu_ctx.scan_config().split(" (")[0]
@@ -86,5 +89,5 @@ def test_autotuner_choice_is_reported_and_kept(gpu_ctx, form):
                                                                          tile_config=chosen[0]))
     assert n3 == n1 and np.array_equal(forced, first)
     with pytest.raises(capi.EpiError) as err:
-        gpu_ctx.scan([(0, 10, 0, 10)], capi.default_opts(form=form, tile_config=N_CANDIDATES + 1))
+        gpu_ctx.scan([(0, 10, 0, 10)], capi.default_opts(form=form, tile_config=nc + 1))
     assert err.value.status == capi.EPI_E_INVALID
