@@ -213,11 +213,12 @@ __global__ void __launch_bounds__(Sh::NT, 1) k_scan_popc(ScanArgs a, const __gri
             for (int st = 0; st < min(RS, nst); ++st) issue(st);
         __syncthreads();  // maj
 
-        // expansion of stage st into buffer b: work item -> (i-SNP, 8 individuals)
+        // expansion of stage st into buffer b: work item -> (i-SNP, 8 individuals), consecutive
+        // threads on consecutive i-SNPs (contiguous stores, the same trait words in a warp)
         auto expand = [&](int st, int b) {
             const int r = st % RS;
             for (int it = tid; it < 8 * TI; it += NT) {
-                const int i = it >> 3, part = it & 7, w = part >> 2, k8 = 8 * (part & 3);
+                const int i = it % TI, part = it / TI, w = part >> 2, k8 = 8 * (part & 3);
                 const uint4 P = sm.raw_i[r][i][w];
                 const int mj = sm.maj[i];
                 const uint32_t PA = mj == 0 ? P.y : P.x, PB = mj == 2 ? P.y : P.z;
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(Sh::NT, 1) k_scan_popc(ScanArgs a, const __gri
                 }
             }
             if (tid < TI * KW) {
-                const int i = tid >> 1, w = tid & 1;
+                const int i = tid % TI, w = tid / TI;
                 const uint4 P = sm.raw_i[r][i][w];
                 const int mj = sm.maj[i];
                 const uint32_t W = __ldg(wt + KW * st + w);
