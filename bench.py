@@ -334,6 +334,8 @@ def main():
     ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
     ap.add_argument("--form", default="auto", choices=["auto", "popc", "tensor"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tile", type=int, default=0,
+                    help="kernel variant of the form (the scan option tile_config; 0 = the autotuner's choice)")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch each scan's device work directly instead of replaying its captured CUDA graph")
     ap.add_argument("--popc-sample", type=int, default=20000,
@@ -364,7 +366,8 @@ def main():
     gname, sms = ctx.device_info()
     gp, y, valid = data["gpack"], data["y"], data["valid"]
     ntraits = data["ntraits"]
-    opts = capi.default_opts(test=test, t1=t1, t2=t2, form=form, report_trait=0, no_graph=int(args.no_graph))
+    opts = capi.default_opts(test=test, t1=t1, t2=t2, form=form, report_trait=0, no_graph=int(args.no_graph),
+                             tile_config=args.tile)
     blocks = data["blocks"]
     pairs_step = sum(block_pairs(b) for b in blocks) * ntraits
 
