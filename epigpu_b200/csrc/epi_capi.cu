@@ -24,7 +24,8 @@ cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int 
                           uint32_t *codes, int Wc, uint8_t *hcodes, uint8_t *h3, uint32_t *missbits,
                           cudaStream_t stream);
 cudaError_t launch_qmiss(const uint32_t *missbits, int nsnp, int Wp, const uint32_t *wmask, const double *qd,
-                        const double *qr, int Np, int ntraits, double *qm, double *rm, cudaStream_t stream);
+                        const double *qr, int Np, int ntraits, double *qm, double *rm, double *nm,
+                        cudaStream_t stream);
 cudaError_t launch_major(const uint4 *planes, int nsnp, int Wp, uint8_t *maj, cudaStream_t stream);
 cudaError_t launch_marg(const uint4 *planes, int nsnp, int Wp, const float *y, const uint32_t *wmask, int Np,
                         int ntraits, double *pmC, int32_t *pmN, double *pmQ, cudaStream_t stream);
@@ -334,12 +335,11 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
             }
         }
     }
-    // tensor form: per valid individual the flag, three balanced base-256 digits of
-    // Y = round(y * 2^sy) (|Y| <= 8355711), the quantised y^2 centred on the middle of its
-    // range, e = (Y 2^-sy)^2 - qcen, and three balanced digits of E = round(e / qstep)
-    // (|E| <= 8355711): the B columns that give the y^2 sum over individuals missing at the
-    // j-SNP. hqd holds e, then the residuals e - E qstep; hsc per trait 2^-sy, qcen, qstep.
-    constexpr int ND = 7;
+    // tensor form: per valid individual the flag and three balanced base-256 digits of
+    // Y = round(y * 2^sy) (|Y| <= 8355711); hqd holds ytilde^2 = (Y 2^-sy)^2 (exact in FP64:
+    // |Y| < 2^23) and Y; hsc per trait 2^-sy, the sum of Y and the number of valid individuals;
+    // hqtot the sum of ytilde^2.
+    constexpr int ND = 4;
     std::vector<int8_t> hd((size_t)ntraits * ND * Np, 0);
     std::vector<double> hqd(2 * (size_t)ntraits * Np, 0.0), hqtot(ntraits, 0.0), hsc(3 * (size_t)ntraits, 1.0);
     for (int t = 0; t < ntraits; ++t) {
@@ -361,7 +361,7 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
         const double scale = std::ldexp(1.0, sy);
         hsc[t] = std::ldexp(1.0, -sy);
         int8_t *d0 = hd.data() + (size_t)t * ND * Np;
-        double qmax = 0.0;
+        long long ysum = 0;
         for (int k = 0; k < nid; ++k) {
             if (!ok(k)) continue;
             long long Y = std::llround(((double)yt[k] - mu) * p2 * scale);
@@ -374,25 +374,12 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
             d0[3 * (size_t)Np + k] = (int8_t)a2;
             const double yq = (double)Y * hsc[t];
             hqd[(size_t)t * Np + k] = yq * yq;
-            qmax = std::max(qmax, yq * yq);
+            hqd[((size_t)ntraits + t) * Np + k] = (double)Y;
+            hqtot[t] += yq * yq;
+            ysum += Y;
         }
-        const double qcen = 0.5 * qmax, qstep = qcen > 0.0 ? qcen / 8355711.0 : 1.0;
-        hsc[ntraits + t] = qcen;
-        hsc[2 * (size_t)ntraits + t] = qstep;
-        for (int k = 0; k < nid; ++k) {
-            if (!ok(k)) continue;
-            const double e = hqd[(size_t)t * Np + k] - qcen;
-            hqd[(size_t)t * Np + k] = e;
-            hqtot[t] += e;
-            long long E = std::llround(e / qstep);
-            E = std::min(8355711LL, std::max(-8355711LL, E));
-            const long long b0 = ((E + 128) & 255) - 128, E1 = (E - b0) / 256;
-            const long long b1 = ((E1 + 128) & 255) - 128, b2 = (E1 - b1) / 256;
-            d0[4 * (size_t)Np + k] = (int8_t)b0;
-            d0[5 * (size_t)Np + k] = (int8_t)b1;
-            d0[6 * (size_t)Np + k] = (int8_t)b2;
-            hqd[((size_t)ntraits + t) * Np + k] = e - (double)E * qstep;
-        }
+        hsc[ntraits + t] = (double)ysum;
+        hsc[2 * (size_t)ntraits + t] = (double)nv;
     }
     size_t need = (size_t)ntraits * Np * sizeof(float);
     size_t cap_y = ctx->traits_cap, cap_q = ctx->traits_cap;
@@ -557,10 +544,10 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     }
     if (r.form == EPI_FORM_TENSOR && !ctx->qm_valid) {
         const size_t tn = (size_t)ctx->ntraits * ctx->nsnp;
-        CK(ensure(&ctx->d_qm, &ctx->qm_cap, 2 * tn * sizeof(double)));
+        CK(ensure(&ctx->d_qm, &ctx->qm_cap, 3 * tn * sizeof(double)));
         CK(epi::launch_qmiss(ctx->d_missbits, ctx->nsnp, ctx->Wp, ctx->d_wmask, ctx->d_qd,
                              ctx->d_qd + (size_t)ctx->ntraits * ctx->Np, ctx->Np, ctx->ntraits, ctx->d_qm,
-                             ctx->d_qm + tn, ctx->stream));
+                             ctx->d_qm + tn, ctx->d_qm + 2 * tn, ctx->stream));
         ctx->qm_valid = true;
     }
     if (r.form == EPI_FORM_POPC && !ctx->pm_valid) {
@@ -582,12 +569,13 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     a.nid = ctx->nid;
     a.nsnp = ctx->nsnp;
     a.yscale = ctx->d_yscale;
-    a.qcen = ctx->d_yscale + ctx->ntraits;
-    a.qstep = ctx->d_yscale + 2 * (size_t)ctx->ntraits;
+    a.ytot = ctx->d_yscale + ctx->ntraits;
+    a.nvalid = ctx->d_yscale + 2 * (size_t)ctx->ntraits;
     a.qd = ctx->d_qd;
     a.qtot = ctx->d_qtot;
     a.qm = ctx->d_qm;
-    a.rm = ctx->d_qm + (size_t)ctx->ntraits * ctx->nsnp;
+    a.sm = ctx->d_qm + (size_t)ctx->ntraits * ctx->nsnp;
+    a.nm = ctx->d_qm + 2 * (size_t)ctx->ntraits * ctx->nsnp;
     a.ydig = ctx->d_ydig;
     a.maj = ctx->d_maj;
     a.pmC = ctx->d_pmC;

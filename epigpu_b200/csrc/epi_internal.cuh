@@ -14,13 +14,13 @@
 // and for the tensor-core form
 //   hcodes  uint8 [nsnp][Np]      one-hot genotype byte: 1 << g for g in 0..2, 0 if missing
 //   missbits uint32 [nsnp][Wp]    missing-genotype bits
-//   ydig    int8 [T][7][Np]       per individual: phenotype-valid flag, the three balanced
-//                                 base-256 digits (low first) of round(y * 2^sy), and three
-//                                 of E = round(e / qstep) (e below)
-//   qd      double [2][T][Np]     e = (quantised y)^2 - qcen[t], then e - qstep[t] * E (the part
-//                                 the two digits do not hold), 0 where invalid; qtot[T] sum of e
-//   qm, rm  double [T][nsnp]      the sums of e and of the residuals over the individuals
-//                                 missing at that SNP
+//   ydig    int8 [T][4][Np]       per individual: phenotype-valid flag and the three balanced
+//                                 base-256 digits (low first) of Y = round(y * 2^sy)
+//   qd      double [2][T][Np]     ytilde^2 (ytilde = Y 2^-sy, the quantised y), then Y itself;
+//                                 0 where invalid; per trait qtot = sum of ytilde^2, ytot = sum
+//                                 of Y, nvalid = count over the valid individuals
+//   qm, sm, nm double [T][nsnp]   the sums of ytilde^2 and of Y, and the count, over the valid
+//                                 individuals missing at that SNP
 // Individuals are padded to Np = 32*Wp (a multiple of 128); padding carries no genotype
 // and no phenotype.
 #pragma once
@@ -74,8 +74,8 @@ struct ScanArgs {
     const uint32_t *wmask;
     const double *qc;          // [T]
     const double *yscale;      // [T] (tensor form: 2^-sy)
-    const double *qd, *qtot, *qm, *rm;
-    const double *qcen, *qstep;  // [T] (tensor form: centre and step of the 16-bit y^2 digits)
+    const double *qd, *qtot, *qm, *sm, *nm;  // tensor form (layout above)
+    const double *ytot, *nvalid;             // [T] (tensor form)
     const int8_t *ydig;
     // plain form: per SNP the most frequent genotype; per (trait, SNP) the FP64 marginals by
     // genotype -- sum of y [T][nsnp][3], count [T][nsnp][3], sum of y^2 over the individuals

@@ -71,27 +71,30 @@ __global__ void k_unpack(const int32_t *__restrict__ raw, int nsnp, int nid, int
 }
 
 // Per trait t and SNP s, over the individuals missing at s (and phenotype-valid for t):
-// qm[t][s] = sum of qd[t][k] and, when qr is given, rm[t][s] = sum of qr[t][k]
+// qm[t][s] = sum of qd[t][k], rm[t][s] = sum of qr[t][k] and nm[t][s] = their number
 __global__ void k_qmiss(const uint32_t *__restrict__ missbits, int nsnp, int Wp, const uint32_t *__restrict__ wmask,
                         const double *__restrict__ qd, const double *__restrict__ qr, int Np, int ntraits,
-                        double *__restrict__ qm, double *__restrict__ rm)
+                        double *__restrict__ qm, double *__restrict__ rm, double *__restrict__ nm)
 {
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= (long long)nsnp * ntraits) return;
     const int t = (int)(gid / nsnp), s = (int)(gid % nsnp);
     double x = 0.0, r = 0.0;
+    int cnt = 0;
     const uint32_t *mb = missbits + (size_t)s * Wp;
     for (int w = 0; w < Wp; ++w) {
         uint32_t bits = mb[w] & wmask[(size_t)t * Wp + w];
+        cnt += __popc(bits);
         while (bits) {
             const size_t k = (size_t)t * Np + 32 * w + __ffs(bits) - 1;
             x += qd[k];
-            if (qr) r += qr[k];
+            r += qr[k];
             bits &= bits - 1;
         }
     }
     qm[gid] = x;
-    if (rm) rm[gid] = r;
+    rm[gid] = r;
+    nm[gid] = (double)cnt;
 }
 
 // Per SNP the most frequent genotype (ties to the lower code), one warp per SNP: the plain
@@ -203,12 +206,13 @@ cudaError_t launch_unpack(const int32_t *raw, int nsnp, int nid, int npack, int 
 }
 
 cudaError_t launch_qmiss(const uint32_t *missbits, int nsnp, int Wp, const uint32_t *wmask, const double *qd,
-                        const double *qr, int Np, int ntraits, double *qm, double *rm, cudaStream_t stream)
+                        const double *qr, int Np, int ntraits, double *qm, double *rm, double *nm,
+                        cudaStream_t stream)
 {
     const long long total = (long long)nsnp * ntraits;
     const int nt = 256;
     k_qmiss<<<(unsigned)((total + nt - 1) / nt), nt, 0, stream>>>(missbits, nsnp, Wp, wmask, qd, qr, Np, ntraits, qm,
-                                                                     rm);
+                                                                     rm, nm);
     return cudaGetLastError();
 }
 

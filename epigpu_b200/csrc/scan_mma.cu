@@ -3,31 +3,29 @@
 // Per pair (i, j) the reference accumulates, over individuals k, the 3x3 genotype-cell
 // counts and phenotype sums (src/EpiOpenCL.c:110-228). Both are contractions over k:
 //     n_ab = sum_k [g_i(k)=a] [g_j(k)=b] w_k        S_ab = sum_k [g_i(k)=a] [g_j(k)=b] y_k
-// so for a tile of 40 i-SNPs x 16 j-SNPs they are one integer GEMM
-//     D[128 x 240] = A[128 x K] * B[K x 240]
+// so for a tile of 40 i-SNPs x 21 j-SNPs they are one integer GEMM
+//     D[128 x 252] = A[128 x K] * B[K x 252]
 //   A rows (row 32w + l, l < 30): i-SNP 10w + l/3, genotype a = l%3: [g_i(k) == a]
-//   B cols (type t, column 16t + j'):
-//     t = 4b + s (t < 12): [g_j(k) == b] * D_s(k), D_0 = w_k (phenotype valid) and D_1..3 the
-//       balanced base-256 digits of the fixed-point phenotype Y_k = round(y_k * 2^sy)
-//       (y centred, 0 when invalid);
-//     t = 12..14: [g_j(k) missing] * E_s(k), the three balanced digits of
-//       E_k = round((ytilde_k^2 - qcen) / qstep), ytilde = Y 2^-sy (0 when invalid).
+//   B cols: type t = 4b + s (b = 0..2 the j genotype, s = 0..3), [g_j(k) == b] * D_s(k), with
+//     D_0 = w_k (phenotype valid) and D_1..3 the balanced base-256 digits of the fixed-point
+//     phenotype Y_k = round(y_k * 2^sy) (y centred, 0 when invalid); column of (t, j') in
+//     the pair MMA: 128 (t / 6) + 21 (t % 6) + j' (each CTA of the pair holds six types).
 // int8 operands, int32 accumulation: counts and digit sums are exact, so
 //     S_ab = (D1 + 256 D2 + 65536 D3) * 2^-sy exactly for the quantised phenotype.
-// The sum of ytilde^2 over the pair's valid individuals (both genotypes known, phenotype
-// valid) is, with e_k = ytilde_k^2 - qcen = qstep E_k + r_k,
-//     Q_ij = qcen * N_ij + (qtot - QM_i) - sum_k [g_i(k) known] [g_j(k) missing] e_k
-// where qtot - QM_i = sum of e over individuals known at i (exact FP64, per SNP), and the
-// last sum is qstep times the t = 12..14 columns summed over a, plus the residuals r over the
-// same individuals, taken as RM_j (r summed over all individuals missing at j, FP64, per
-// SNP). The one approximation: the residuals of individuals missing at both SNPs are counted
-// in RM_j, an error of at most qstep / 2 per such individual (qstep = max(ytilde^2) / 2^24).
-// The epilogue screens F and F2 in FP32 from the exact integer cells and forms SSB / SSI /
-// F / F2 in FP64 for every pair that could be a hit or a new maximum.
+// The sum of ytilde^2 (ytilde = Y 2^-sy) over the pair's valid individuals (both genotypes
+// known, phenotype valid) follows from per-SNP sums over each SNP's missing individuals:
+//     Q_ij = Qtot - QM_i - QM_j + QMM_ij,   QMM_ij = sum of ytilde^2 over the individuals
+// missing at both SNPs, 0 <= QMM_ij. Their number and Y sum are exact from the cells:
+//     n_mm = N_ij - Nvalid + NM_i + NM_j,   Y_mm = St_ij - Ytot + SM_i + SM_j,
+// so QMM_ij = 0 when n_mm = 0 and (Y_mm 2^-sy)^2 when n_mm = 1 (exact); only a pair with two
+// or more such individuals that needs exact statistics intersects the two SNPs' missing bits.
+// The epilogue screens F and F2 in FP32 with Q_ij >= Qtot - QM_i - QM_j (F and F2 fall as Q
+// grows, so the screen bounds them from above) and forms SSB / SSI / F / F2 in FP64 for every
+// pair that could be a hit or a new maximum.
 //
 // The GEMM runs on a CTA pair (a cluster of two CTAs on two SMs, tcgen05 cta_group::2): one
 // MMA of M = 256 rows (each CTA's 40 i-SNPs, 3 genotype rows each, in its own shared memory)
-// by N = 256 columns (the 240 columns of 16 j-SNPs plus 16 zero columns; each CTA holds and
+// by N = 256 columns (the 252 columns of 21 j-SNPs plus 4 zero columns; each CTA holds and
 // builds half of them), so each SM expands half of B per stage. Each CTA's TMEM receives the
 // accumulator rows of its own i-SNPs, which its epilogue reads.
 //
@@ -37,13 +35,13 @@
 // Per CTA, 15 warps:
 //   warp 13       A loader (one thread): per 128-individual stage, the CTA's A stage (four
 //                 2-D tiled loads of 30 h3 rows into rows 32w..32w+29); no multicast
-//   warp 14       raw loader (one thread): per stage, the j-tile's 16 one-hot rows and the
-//                 trait's 7 digit rows, up to RSTAGES stages ahead of the B producers
+//   warp 14       raw loader (one thread): per stage, the j-tile's 21 one-hot rows and the
+//                 trait's 4 digit rows, up to RSTAGES stages ahead of the B producers
 //   warps 4-7     B producers: raw rows -> this CTA's half of the B stage (K-major, 128-byte
-//                 swizzle): CTA 0 column types 0-7, CTA 1 types 8-14
+//                 swizzle): CTA 0 column types 0-5, CTA 1 types 6-11
 //   warp 12       CTA 0: MMA issuer (one thread): 4 pair MMAs per stage; CTA 1: forwards the
 //                 completion of its own A stages to CTA 0. Both: TMEM allocation (pair form)
-//   warps 0-3, 8-11  epilogue, two warps per TMEM lane quarter, three j rounds each
+//   warps 0-3, 8-11  epilogue, two warps per TMEM lane quarter, seven j rounds between them
 // Handshakes: CTA 0's bfull / afull / acc_empty barriers also count arrivals from CTA 1; the
 // MMA's commits arrive on both CTAs' aempty, bempty and acc_full barriers (multicast). TMEM (512
 // columns per CTA): accumulators at [0, 256) and [256, 512). All waits are bounded
@@ -64,33 +62,42 @@ namespace mma {
 
 constexpr int TI = 40;         // i-SNPs per CTA (4 lane quarters x 10 triplets)
 constexpr int TIP = 2 * TI;    // i-SNPs per pair tile
-constexpr int TJ = 16;         // j-SNPs per tile
-constexpr int NTY = 12;        // B column types per j-SNP: b (3) x {w, d0, d1, d2} ...
-constexpr int NTYPE = 15;      // ... and missing x {e0, e1, e2}
-constexpr int NCOL = TJ * NTYPE;  // 240 columns in use
-constexpr int N = 256;         // MMA width (pair MMAs take multiples of 32); columns 240-255 zero
+constexpr int TJ = 21;         // j-SNPs per tile
+constexpr int NTYPE = 12;      // B column types per j-SNP: b (3) x {w, d0, d1, d2}
+constexpr int NCOL = TJ * NTYPE;  // 252 columns in use
+constexpr int N = 256;         // MMA width (pair MMAs take multiples of 32)
 constexpr int NH = N / 2;      // B columns held by each CTA
+constexpr int TYH = NTYPE / 2; // column types held by each CTA (6 x 21 = 126 of its 128 rows)
 constexpr int M = 256;         // MMA height over the pair
 constexpr int KS = 128;        // individuals per pipeline stage
-constexpr int ND = 7;          // digit rows per trait: w, Y digits (3), E digits (3)
+constexpr int ND = 4;          // digit rows per trait: w, Y digits (3)
 constexpr int ROUNDS = (TJ + 2) / 3;  // j rounds of the epilogue (3 j-SNPs per round)
 constexpr uint32_t ACC_COL1 = N;
 __host__ __device__ constexpr uint32_t acc_col(uint32_t buf) { return buf ? ACC_COL1 : 0u; }
+// accumulator column of column type ty, j-SNP jj of the tile
+__host__ __device__ constexpr int bcol(int ty, int jj) { return (ty / TYH) * NH + (ty % TYH) * TJ + jj; }
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int A_STAGE = (M / 2) * KS;  // 16 KB
 constexpr int B_STAGE = NH * KS;       // 16 KB
 constexpr int A_BOX = 30;              // h3 rows per TMA box (10 i-SNPs x 3 genotypes)
 constexpr uint32_t A_BYTES = 4 * A_BOX * KS;  // transaction bytes per A stage (one CTA)
 // raw stage: the j-tile's one-hot rows and the trait's digit rows, 1024-aligned sections
-constexpr int RAW_J = 0, RAW_D = TJ * KS;
+constexpr int RAW_J = 0, RAW_D = (TJ * KS + 1023) / 1024 * 1024;
 constexpr int RAW_STAGE = 4 * 1024;
 constexpr uint32_t RAW_BYTES = (TJ + ND) * KS;
+// producer work items per stage: (j-SNP, 16-individual chunk); 128 producer threads take the
+// first 128 and the threads below XTRA one more (the j-SNPs 16..20, same chunk)
+constexpr int XTRA = TJ * 8 - 128;
 
 constexpr uint32_t IDESC = tc::idesc_i8(M, N);
 static_assert(RAW_D % 1024 == 0 && RAW_D + ND * KS <= RAW_STAGE, "raw layout");
 static_assert(B_STAGE % 1024 == 0 && A_STAGE % 1024 == 0 && N % 32 == 0 && N <= 256 && NCOL <= N, "operand tiles");
-static_assert(NCOL - NH == 7 * TJ && NH == 8 * TJ, "B split: CTA 0 types 0-7, CTA 1 types 8-14 + padding");
-static_assert(2 * N <= (int)TMEM_COLS && ROUNDS % 6 == 0, "TMEM layout / epilogue split");
+static_assert(NTYPE % 2 == 0 && TYH * TJ <= NH && TYH == 6, "B split: CTA 0 types 0-5, CTA 1 types 6-11");
+static_assert(XTRA >= 0 && XTRA <= 128 && (XTRA % 8) == 0 && 16 + XTRA / 8 == TJ, "producer items");
+static_assert(2 * N <= (int)TMEM_COLS, "TMEM layout: two accumulators");
+// the x4 accumulator loads of a round's three j-SNPs read one column past them: within the
+// pair's 256 columns even for the last type of each half
+static_assert(bcol(NTYPE - 1, 3 * (ROUNDS - 1)) + 3 < N && bcol(TYH - 1, 3 * (ROUNDS - 1)) + 3 < NH, "epilogue loads");
 
 // Ring depths (a kernel variant, chosen by the autotuner): A stages come by TMA from L2 / DRAM
 // and need the deeper ring; B stages are built from raw rows already in shared memory; the raw
@@ -330,12 +337,12 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
         tc::tmem_alloc_pair(&sm.tmem_base, TMEM_COLS);
         tc::tmem_relinquish_pair();
     }
-    // CTA 1 holds B columns 128-255: its rows 112-127 (columns 240-255) stay zero
-    if (rank == 1)
-        for (int w = threadIdx.x; w < BSTAGES * (NH - (NCOL - NH)) * 8; w += blockDim.x) {
-            const int st = w / ((NH - (NCOL - NH)) * 8), n = (NCOL - NH) + (w / 8) % (NH - (NCOL - NH)), c = w % 8;
-            *reinterpret_cast<uint4 *>(sm.b[st] + (n >> 3) * 1024 + (n & 7) * 128 + c * 16) = make_uint4(0, 0, 0, 0);
-        }
+    // each CTA's B half holds six column types in rows 0-125: rows 126-127 stay zero
+    constexpr int ZR = NH - TYH * TJ;
+    for (int w = threadIdx.x; w < BSTAGES * ZR * 8; w += blockDim.x) {
+        const int st = w / (ZR * 8), n = TYH * TJ + (w / 8) % ZR, c = w % 8;
+        *reinterpret_cast<uint4 *>(sm.b[st] + (n >> 3) * 1024 + (n & 7) * 128 + c * 16) = make_uint4(0, 0, 0, 0);
+    }
     tc::fence_proxy_async_smem();
     // maxima of F and F2 per trait: per CTA in shared memory (flushed to global memory once,
     // at the end) up to SMAX_TRAITS traits, else the global maxima directly
@@ -383,7 +390,9 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
     }
     if (warp >= 4 && warp < 8) {
         // ---------------- B producers: thread -> (j-SNP, 16-individual chunk) ----------------
+        // items (jj, c) with jj < 16 for every thread, and (16 + t/8, c) for t < XTRA
         const int t = threadIdx.x - 128, jj = t >> 3, c = t & 7;
+        const bool xtra = t < XTRA;
         uint32_t stage = 0, phase = 0, rs = 0, rph = 0;
         bool ok = true;
         for (long long u = pair; u < units && ok; u += npairs) {
@@ -396,11 +405,15 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                     break;
                 }
                 const uint8_t *raw = sm.raw[rs];
-                const uint4 h = ld_sw128(raw + RAW_J, jj, c);
                 uint8_t *base = sm.b[stage];
-                // column type ty of this CTA's half at local row (ty - 8 rank) * 16 + jj
-                auto put = [&](int ty, const uint4 &m, const uint4 &dv) {
-                    const int n = (ty - 8 * (int)rank) * TJ + jj;
+                uint4 d[ND];
+#pragma unroll
+                for (int s2 = 0; s2 < ND; ++s2) d[s2] = ld_sw128(raw + RAW_D, s2, c);
+                // column type ty (genotype ty / 4, digit row ty % 4) of j-SNP jx at local row
+                // (ty - 6 rank) * 21 + jx
+                auto put = [&](int ty, int jx, const uint4 &m) {
+                    const int n = (ty - TYH * (int)rank) * TJ + jx;
+                    const uint4 &dv = d[ty & 3];
                     uint4 o;
                     o.x = m.x & dv.x;
                     o.y = m.y & dv.y;
@@ -408,44 +421,35 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                     o.w = m.w & dv.w;
                     *reinterpret_cast<uint4 *>(base + (n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4)) = o;
                 };
-                if (rank == 0) {
-                    // types 0-7: genotypes 0 and 1 x {w, d0, d1, d2}
-                    uint4 d[4];
-#pragma unroll
-                    for (int s2 = 0; s2 < 4; ++s2) d[s2] = ld_sw128(raw + RAW_D, s2, c);
-#pragma unroll
-                    for (int b = 0; b < 2; ++b) {
-                        uint4 m;
-                        m.x = ((h.x >> b) & 0x01010101u) * 0xFFu;
-                        m.y = ((h.y >> b) & 0x01010101u) * 0xFFu;
-                        m.z = ((h.z >> b) & 0x01010101u) * 0xFFu;
-                        m.w = ((h.w >> b) & 0x01010101u) * 0xFFu;
-#pragma unroll
-                        for (int s2 = 0; s2 < 4; ++s2) put(4 * b + s2, m, d[s2]);
-                    }
-                } else {
-                    // types 8-11: genotype 2 x {w, d0, d1, d2}; 12-14: missing x {e0, e1, e2}
-                    uint4 d[ND];
-#pragma unroll
-                    for (int s2 = 0; s2 < ND; ++s2) d[s2] = ld_sw128(raw + RAW_D, s2, c);
+                // byte mask of genotype b: one-hot bit b of each byte spread to 0xFF
+                auto gmask = [](const uint4 &h, int b) {
                     uint4 m;
-                    m.x = ((h.x >> 2) & 0x01010101u) * 0xFFu;
-                    m.y = ((h.y >> 2) & 0x01010101u) * 0xFFu;
-                    m.z = ((h.z >> 2) & 0x01010101u) * 0xFFu;
-                    m.w = ((h.w >> 2) & 0x01010101u) * 0xFFu;
+                    m.x = ((h.x >> b) & 0x01010101u) * 0xFFu;
+                    m.y = ((h.y >> b) & 0x01010101u) * 0xFFu;
+                    m.z = ((h.z >> b) & 0x01010101u) * 0xFFu;
+                    m.w = ((h.w >> b) & 0x01010101u) * 0xFFu;
+                    return m;
+                };
+                auto build = [&](int jx) {
+                    const uint4 h = ld_sw128(raw + RAW_J, jx, c);
+                    if (rank == 0) {
+                        // types 0-5: genotype 0 x {w, d0, d1, d2}, genotype 1 x {w, d0}
+                        const uint4 m0 = gmask(h, 0), m1 = gmask(h, 1);
 #pragma unroll
-                    for (int s2 = 0; s2 < 4; ++s2) put(8 + s2, m, d[s2]);
-                    // missing genotype: one-hot byte 0 (bits 0-2 clear); the shifts only move
-                    // bits of the next byte into bits 6-7 of this one, which the mask drops
-                    uint4 mm;
-                    mm.x = (((h.x | (h.x >> 1) | (h.x >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
-                    mm.y = (((h.y | (h.y >> 1) | (h.y >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
-                    mm.z = (((h.z | (h.z >> 1) | (h.z >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
-                    mm.w = (((h.w | (h.w >> 1) | (h.w >> 2)) & 0x01010101u) ^ 0x01010101u) * 0xFFu;
-                    put(12, mm, d[4]);
-                    put(13, mm, d[5]);
-                    put(14, mm, d[6]);
-                }
+                        for (int ty = 0; ty < 4; ++ty) put(ty, jx, m0);
+                        put(4, jx, m1);
+                        put(5, jx, m1);
+                    } else {
+                        // types 6-11: genotype 1 x {d1, d2}, genotype 2 x {w, d0, d1, d2}
+                        const uint4 m1 = gmask(h, 1), m2 = gmask(h, 2);
+                        put(6, jx, m1);
+                        put(7, jx, m1);
+#pragma unroll
+                        for (int ty = 8; ty < 12; ++ty) put(ty, jx, m2);
+                    }
+                };
+                build(jj);
+                if (xtra) build(16 + jj);
                 // the raw slot is released only after the stores above, which consume every
                 // value loaded from it (an arrive right after the loads can overtake them)
                 tc::fence_proxy_async_smem();
@@ -460,9 +464,10 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
             }
         }
     } else if (epi_warp) {
-        // ---------------- epilogue: warps 0-3 rounds 0-2, warps 8-11 rounds 3-5 ----------------
-        constexpr int RPW = ROUNDS / EPW;  // j rounds per epilogue warp
-        const int e = warp & 3, rho0 = (warp < 4 ? 0 : (warp < 12 ? 1 : 2)) * RPW;
+        // ---------------- epilogue: the j rounds split over the warps of each lane quarter ----------------
+        // warps 0-3 (group 0), 8-11 (group 1), 16-19 (group 2): rounds [rb(g), rb(g + 1))
+        const int e = warp & 3, grp = warp < 4 ? 0 : (warp < 12 ? 1 : 2);
+        const int rho_begin = (grp * ROUNDS + EPW - 1) / EPW, rho_end = ((grp + 1) * ROUNDS + EPW - 1) / EPW;
         const int ii = 10 * e + lane / 3, ga = lane % 3, tbase = (lane / 3) * 3;
         const bool rowok = lane < 30;
         const uint32_t tl = tmem + ((uint32_t)(32 * e) << 16);
@@ -473,12 +478,16 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
             if (un.skip) continue;
             un.i0 += TI * (int)rank;  // this CTA's i-SNPs
             const int t = un.trait;
-            const double sc = a.yscale[t], qcen = a.qcen[t], qstep = a.qstep[t];
+            const double sc = a.yscale[t];
             const int di = un.i0 + ii;
             const bool ivalid = rowok && di < un.bd.size1;
             const int gi = un.bd.start1 + (ivalid ? di : 0);
-            // sum of (ytilde^2 - qcen) over the individuals known at SNP i
-            const double pki = ivalid ? a.qtot[t] - a.qm[(size_t)t * a.nsnp + gi] : 0.0;
+            const size_t mi = (size_t)t * a.nsnp + gi;
+            // sum of ytilde^2 over the valid individuals known at SNP i; and the quantities of
+            // the individuals missing at i that the exact path needs
+            const double pki = ivalid ? a.qtot[t] - a.qm[mi] : 0.0;
+            const double smi = ivalid ? a.sm[mi] : 0.0, nmi_nv = ivalid ? a.nm[mi] - a.nvalid[t] : 0.0;
+            const double ytot = a.ytot[t];
             if (!tc::mbar_wait(&sm.acc_full[buf], accph[buf], abort, a.wait_ns)) {
                 fail(a, sm, 3);
                 break;
@@ -488,7 +497,6 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
             const bool report = a.report_trait < 0 || a.report_trait == t;
             const bool dumping = t == a.report_trait && (a.dump_counts || a.dump_F);
             const float t1c = screen_lo(a.t1), t2c = screen_lo(a.t2), scf = (float)sc;
-            const float qcenf = (float)qcen, qstepf = (float)qstep, pkif = (float)pki;
             unsigned int fmx = 0u, f2mx = 0u;  // this thread's largest F, F2 of the tile (encoded)
             // screen against the CTA's maxima so far (exact values, a lower bound of the final
             // maxima): a pair that can raise a maximum always takes the exact path
@@ -496,25 +504,27 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
             const unsigned int m2 = reinterpret_cast<volatile unsigned int *>(mxf2)[t];
             float fmx_f = m1 ? ord2f(m1) : -INFINITY, f2mx_f = m2 ? ord2f(m2) : -INFINITY;
 #pragma unroll 1
-            for (int rho = rho0; rho < rho0 + RPW; ++rho) {
+            for (int rho = rho_begin; rho < rho_end; ++rho) {
                 const int jb = 3 * rho;
                 const int jl = jb + ga;
                 const int dj = un.j0 + jl;
                 const bool valid = ivalid && (jl < TJ) && dj < un.bd.size2 &&
                                    (un.bd.start1 + di > un.bd.start2 + dj);
-                const double rmj = valid ? a.rm[(size_t)t * a.nsnp + un.bd.start2 + dj] : 0.0;
+                const int gj = un.bd.start2 + (valid ? dj : 0);
+                const size_t mj = (size_t)t * a.nsnp + gj;
+                const double qmj = valid ? a.qm[mj] : 0.0;
                 uint32_t v[NTYPE][4];
 #pragma unroll
                 for (int ty = 0; ty < NTYPE; ++ty)
-                    tc::tmem_ld4(acc + ty * TJ + jb, v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
+                    tc::tmem_ld4(acc + bcol(ty, jb), v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
                 tc::tmem_wait_ld();
                 // this lane's accumulator row (SNP i, genotype ga) folded per column c of the round
-                // (j-SNP jb + c): three counts, three FP32 phenotype sums and the FP32 sum of E.
-                // Up to 131,072 individuals every digit sum is below 2^24 in magnitude, so the
-                // conversions are exact and the two fmas round once each (beyond, the conversions
-                // round too: relative 2^-24, far inside the screen's margin).
+                // (j-SNP jb + c): three counts and three FP32 phenotype sums. Up to 131,072
+                // individuals every digit sum is below 2^24 in magnitude, so the conversions are
+                // exact and the two fmas round once each (beyond, the conversions round too:
+                // relative 2^-24, far inside the screen's margin).
                 int cn[3][3];
-                float cs[3][3], ce[3];
+                float cs[3][3];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
 #pragma unroll
@@ -523,8 +533,6 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                         cs[c][b] = fmaf(65536.0f, (float)(int)v[4 * b + 3][c],
                                         fmaf(256.0f, (float)(int)v[4 * b + 2][c], (float)(int)v[4 * b + 1][c]));
                     }
-                    ce[c] = fmaf(65536.0f, (float)(int)v[NTY + 2][c],
-                                 fmaf(256.0f, (float)(int)v[NTY + 1][c], (float)(int)v[NTY][c]));
                 }
                 // the pair (SNP i, j-SNP jb + ga) is this lane's: its own row directly, the rows of
                 // the triplet's other two lanes by shuffle, each lane offering the column its reader
@@ -544,10 +552,6 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                     sfd[3 + b] = __shfl_sync(0xffffffffu, pick3(cs[0][b], cs[1][b], cs[2][b], o1), s1);
                     sfd[6 + b] = __shfl_sync(0xffffffffu, pick3(cs[0][b], cs[1][b], cs[2][b], o2), s2);
                 }
-                // E sum over individuals known at i (the three rows) and missing at j
-                const float emf = pick3(ce[0], ce[1], ce[2], ga) +
-                                  __shfl_sync(0xffffffffu, pick3(ce[0], ce[1], ce[2], o1), s1) +
-                                  __shfl_sync(0xffffffffu, pick3(ce[0], ce[1], ce[2], o2), s2);
                 PairStat s;
                 s.nfac = s.d1 = s.d2 = 0;
                 s.F = s.F2 = 0.0;
@@ -556,7 +560,9 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                 if (valid) {
 #pragma unroll
                     for (int c = 0; c < 9; ++c) npair += n[c];
-                    const float Qf = fmaf(qcenf, (float)npair, pkif) - fmaf(qstepf, emf, (float)rmj);
+                    // a lower bound of the pair's sum of squares (QMM_ij >= 0 left out), so the
+                    // screened F and F2 bound the pair's values from above
+                    const float Qf = (float)(pki - qmj);
                     float Ff, F2f;
                     pair_stat_f32(n, sfd, scf, Qf, a.test_int != 0, Ff, F2f);
                     exact = dumping || npair < 256 || !(Ff <= t1c) || !(Ff <= screen_lo(fmx_f)) ||
@@ -579,7 +585,7 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                     // accumulator (still in TMEM until this warp releases it)
 #pragma unroll
                     for (int ty = 0; ty < NTYPE; ++ty)
-                        tc::tmem_ld4(acc + ty * TJ + jb, v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
+                        tc::tmem_ld4(acc + bcol(ty, jb), v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
                     tc::tmem_wait_ld();
                     uint32_t r1[NTYPE], r2[NTYPE];
 #pragma unroll
@@ -587,28 +593,54 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                         r1[ty] = __shfl_sync(0xffffffffu, sel3(v[ty], o1), s1);
                         r2[ty] = __shfl_sync(0xffffffffu, sel3(v[ty], o2), s2);
                     }
+                    double si[9];  // digit sums as exact integers
+                    double qmm = 0.0;
+                    int nmm = 0;
                     if (exact) {
-                        double si[9];  // digit sums as exact integers
+                        double st = 0.0;
 #pragma unroll
                         for (int b = 0; b < 3; ++b) {
                             const uint32_t c1[3] = {sel3(v[4 * b + 1], ga), r1[4 * b + 1], r2[4 * b + 1]};
                             const uint32_t c2[3] = {sel3(v[4 * b + 2], ga), r1[4 * b + 2], r2[4 * b + 2]};
                             const uint32_t c3[3] = {sel3(v[4 * b + 3], ga), r1[4 * b + 3], r2[4 * b + 3]};
 #pragma unroll
-                            for (int r = 0; r < 3; ++r)
+                            for (int r = 0; r < 3; ++r) {
                                 si[3 * r + b] = fma(65536.0, (double)(int)c3[r],
                                                     fma(256.0, (double)(int)c2[r], (double)(int)c1[r]));
+                                st += si[3 * r + b];
+                            }
                         }
-                        long long em = 0;
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) {
-                            const long long sd = (long long)(int)sel3(v[NTY + d], ga) + (long long)(int)r1[NTY + d] +
-                                                 (long long)(int)r2[NTY + d];
-                            em += sd * (1LL << (8 * d));
+                        // the individuals missing at both SNPs: their number, and for a single
+                        // one its y^2 from the Y sums (every term an exact integer below 2^53)
+                        nmm = npair + (int)(nmi_nv + a.nm[mj]);
+                        if (nmm == 1) {
+                            const double ymm = (st - ytot + smi + a.sm[mj]) * sc;
+                            qmm = ymm * ymm;
                         }
-                        const double Q = fma(qcen, (double)npair, pki) - fma(qstep, (double)em, rmj);
-                        s = pair_stat_exact(n, si, sc, Q, a.test_int != 0);
                     }
+                    // two or more: the whole warp intersects the two SNPs' missing bits for each
+                    // such pair in turn and sums ytilde^2 over the intersection
+                    unsigned int need = __ballot_sync(0xffffffffu, exact && nmm >= 2);
+                    while (need) {
+                        const int src = __ffs(need) - 1;
+                        need &= need - 1;
+                        const int si_ = __shfl_sync(0xffffffffu, gi, src), sj_ = __shfl_sync(0xffffffffu, gj, src);
+                        const uint32_t *mbi = a.missbits + (size_t)si_ * a.Wp, *mbj = a.missbits + (size_t)sj_ * a.Wp;
+                        const uint32_t *wm = a.wmask + (size_t)t * a.Wp;
+                        const double *qdt = a.qd + (size_t)t * a.Np;
+                        double part = 0.0;
+                        for (int w = lane; w < a.Wp; w += 32) {
+                            uint32_t bits = mbi[w] & mbj[w] & wm[w];
+                            while (bits) {
+                                part += qdt[32 * w + __ffs(bits) - 1];
+                                bits &= bits - 1;
+                            }
+                        }
+#pragma unroll
+                        for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+                        if (lane == src) qmm = part;
+                    }
+                    if (exact) s = pair_stat_exact(n, si, sc, pki - qmj + qmm, a.test_int != 0);
                 }
                 if (valid && dumping) {
                     const size_t o = (size_t)di * un.bd.size2 + dj;
