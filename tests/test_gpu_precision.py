@@ -75,6 +75,36 @@ def test_f_error_low_call_rate_individuals(gpu_ctx, form):
 
 
 @pytest.mark.parametrize("form", [capi.FORM_POPC, capi.FORM_TENSOR], ids=["popc", "tensor"])
+def test_hits_low_call_rate_individuals(gpu_ctx, form):
+    """The same missingness pattern through the screened scan path (no dump): thresholds at
+    the oracle's 99th and 99.5th percentiles put thousands of pairs near them, and the pairs
+    sharing several individuals missing at both SNPs (one an outlier) must still give the
+    oracle's hit list. The tensor form screens with a lower bound of the pair's sum of
+    squares and takes the exact one only for candidates."""
+    nid, nsnp = 2000, 300
+    rng = np.random.default_rng(61)
+    codes = synth.genotype_codes(nid, nsnp, seed=62, miss=0.005)
+    low = rng.choice(nid, 48, replace=False)
+    codes[:, low] = np.where(rng.random((nsnp, low.size)) < 0.5, 3, codes[:, low])
+    y = ((rng.gamma(1.5, 1.0, nid) - 1.5)).astype(np.float32)
+    y[low[0]] = 25.0
+    phen = np.where(rng.random(nid) < 0.02, np.float32(-9.0), y).astype(np.float32)
+    blk = (0, nsnp, 0, nsnp)
+    _, _, pb0 = oracles.oracle_scan_block(codes, phen, blk, test="i", t1=-1e30, t2=-1e30, per_pair=True)
+    tri = np.tril(np.ones((nsnp, nsnp), bool), -1)
+    t1 = float(np.quantile(pb0["F"][tri], 0.99))
+    t2 = float(np.quantile(pb0["F2"][tri], 0.995))
+    hb, _, pb = oracles.oracle_scan_block(codes, phen, blk, test="i", t1=t1, t2=t2, per_pair=True)
+    near = parity.near_threshold(pb, blk, t1, t2, "i", 1e-4)
+    gpu_ctx.load_packed(synth.pack(codes), nid)
+    gpu_ctx.set_phenotype(phen)
+    got, total, _ = gpu_ctx.scan([blk], capi.default_opts(test="i", t1=t1, t2=t2, form=form))
+    assert total > 400
+    ok, msg = parity.compare_hit_lists(got, hb, near)
+    assert ok, msg
+
+
+@pytest.mark.parametrize("form", [capi.FORM_POPC, capi.FORM_TENSOR], ids=["popc", "tensor"])
 @pytest.mark.parametrize("test", ["f", "i"])
 def test_near_perfect_fit_is_a_hit(gpu_ctx, form, test):
     """A phenotype almost fully determined by one SNP pair's 3x3 genotype cells (noise 1e-6
