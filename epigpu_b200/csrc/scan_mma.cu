@@ -250,6 +250,14 @@ __device__ __forceinline__ PairStat pair_stat_exact(const int n[9], const double
     return r;
 }
 
+// approximate reciprocal of the screen (one MUFU operation, relative error ~2^-23; 1/0 = +inf)
+__device__ __forceinline__ float rcp_fast(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // The same statistics in FP32, as a screen: relative error ~1e-6 for the centred trait and
 // the exact integer cells this gets (no cancellation beyond SSW = Q - ... at large N).
 // A pair whose screened F and F2 are clearly below every threshold and below the running
@@ -266,11 +274,11 @@ __device__ __forceinline__ void pair_stat_f32(const int n[9], const float sd[9],
         St += sf[c];
         nfac += n[c] > 0 ? 1.0f : 0.0f;
     }
-    const float m = St * __frcp_rn(N);
+    const float m = St * rcp_fast(N);
     float mc[9], SSB = 0.0f;
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
-        mc[c] = n[c] > 0 ? sf[c] * __frcp_rn((float)n[c]) : 0.0f;
+        mc[c] = n[c] > 0 ? sf[c] * rcp_fast((float)n[c]) : 0.0f;
         const float d = mc[c] - m;
         SSB = fmaf((float)n[c] * d, d, SSB);
     }
@@ -284,7 +292,7 @@ __device__ __forceinline__ void pair_stat_f32(const int n[9], const float sd[9],
         return;
     }
     const float d1 = nfac - 1.0f, d2 = N - nfac;
-    F = (SSB * d2) / (SSW * d1);
+    F = (SSB * d2) * rcp_fast(SSW * d1);
     F2 = 0.0f;
     if (want_int) {
         float row[3], col[3];
@@ -292,8 +300,8 @@ __device__ __forceinline__ void pair_stat_f32(const int n[9], const float sd[9],
         for (int i = 0; i < 3; ++i) {
             const float rn = (float)(n[3 * i] + n[3 * i + 1] + n[3 * i + 2]);
             const float cn = (float)(n[i] + n[i + 3] + n[i + 6]);
-            row[i] = rn > 0.0f ? (sf[3 * i] + sf[3 * i + 1] + sf[3 * i + 2]) * __frcp_rn(rn) : 0.0f;
-            col[i] = cn > 0.0f ? (sf[i] + sf[i + 3] + sf[i + 6]) * __frcp_rn(cn) : 0.0f;
+            row[i] = rn > 0.0f ? (sf[3 * i] + sf[3 * i + 1] + sf[3 * i + 2]) * rcp_fast(rn) : 0.0f;
+            col[i] = cn > 0.0f ? (sf[i] + sf[i + 3] + sf[i + 6]) * rcp_fast(cn) : 0.0f;
         }
         float SSI = 0.0f;
 #pragma unroll
@@ -301,7 +309,7 @@ __device__ __forceinline__ void pair_stat_f32(const int n[9], const float sd[9],
             const float t = mc[c] - row[c / 3] - col[c % 3] + m;
             SSI = n[c] > 0 ? fmaf((float)n[c] * t, t, SSI) : SSI;
         }
-        F2 = (SSI * d2) / (4.0f * SSW);
+        F2 = (SSI * d2) * rcp_fast(4.0f * SSW);
     }
 }
 
