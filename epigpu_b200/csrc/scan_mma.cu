@@ -42,8 +42,11 @@
 //   warp 12       CTA 0: MMA issuer (one thread): 4 pair MMAs per stage; CTA 1: forwards the
 //                 completion of its own A stages to CTA 0. Both: TMEM allocation (pair form)
 //   warps 0-3, 8-11  epilogue, two warps per TMEM lane quarter, seven j rounds between them
-// Handshakes: CTA 0's bfull / afull / acc_empty barriers also count arrivals from CTA 1; the
-// MMA's commits arrive on both CTAs' aempty, bempty and acc_full barriers (multicast). TMEM (512
+// Handshakes: one operand ring (an A stage and a B stage per slot). CTA 0's `full` barrier of a
+// slot counts its own A load, CTA 1's forward of its A load and the 8 producer warps of both
+// CTAs, so the MMA issuer waits once per stage; its commit arrives on both CTAs' `empty`
+// barrier of the slot (multicast), which the A loaders and producers wait on. CTA 0's acc_empty
+// also counts CTA 1's epilogue warps; commits arrive on both CTAs' acc_full. TMEM (512
 // columns per CTA): accumulators at [0, 256) and [256, 512). All waits are bounded
 // (tc_ptx.cuh); a timeout sets counters[2] and every role leaves its loop; the CTAs meet in
 // a cluster barrier before the TMEM is released.
@@ -99,31 +102,34 @@ static_assert(2 * N <= (int)TMEM_COLS, "TMEM layout: two accumulators");
 // pair's 256 columns even for the last type of each half
 static_assert(bcol(NTYPE - 1, 3 * (ROUNDS - 1)) + 3 < N && bcol(TYH - 1, 3 * (ROUNDS - 1)) + 3 < NH, "epilogue loads");
 
-// Ring depths (a kernel variant, chosen by the autotuner): A stages come by TMA from L2 / DRAM
-// and need the deeper ring; B stages are built from raw rows already in shared memory; the raw
-// ring (j one-hot and digit rows, by TMA) lets the raw loader run ahead of the B producers.
+// Ring depths (a kernel variant, chosen by the autotuner): STAGES operand slots, each an A stage
+// (TMA from L2 / DRAM) and a B stage (built from raw rows already in shared memory), and the raw
+// ring (j one-hot and digit rows, by TMA), which lets the raw loader run ahead of the B
+// producers. One barrier pair per operand slot keeps the MMA issuer's work per stage to one
+// wait and one commit: the issuer is the pipeline's critical path (a barrier wait costs about a
+// hundred cycles even when the barrier is ready).
 //
 // EPW epilogue warps per TMEM lane quarter: 2 (15 warps: epilogue 0-3 and 8-11) or 3 (20 warps:
 // epilogue also 16-19, warp 15 idle). With 3, the 640 threads launch with 96 registers each
 // and the warpgroups rebalance (setmaxnreg): the three epilogue warpgroups to 128, the B
 // producers to 56, the loaders and MMA issuer to 40 -- 3 x 128 x 128 + 128 x 56 + 128 x 40
 // = 61,440 = 640 x 96, the launch's pool.
-template <int AS, int BS, int RSx, int EPW_ = 2>
+template <int S, int RSx, int EPW_ = 2>
 struct Rings {
-    static constexpr int ASTAGES = AS, BSTAGES = BS, RSTAGES = RSx, EPW = EPW_;
+    static constexpr int STAGES = S, RSTAGES = RSx, EPW = EPW_;
     static constexpr int NWARPS = EPW == 2 ? 15 : 20;
     static constexpr int NTHREADS = NWARPS * 32;
     static_assert(EPW == 2 || EPW == 3, "epilogue warps per lane quarter");
     static_assert(EPW == 2 || 3 * 128 * 128 + 128 * 56 + 128 * 40 == NTHREADS * 96, "register split");
     struct Smem {
-        uint8_t a[ASTAGES][A_STAGE];
-        uint8_t b[BSTAGES][B_STAGE];
+        uint8_t a[STAGES][A_STAGE];
+        uint8_t b[STAGES][B_STAGE];
         uint8_t raw[RSTAGES][RAW_STAGE];
-        // bfull: B halves built (CTA 0: 4 local + 4 remote producer warps); afull: A stages landed
-        // (CTA 0: own TMA + CTA 1's forward; CTA 1: own TMA); aempty / bempty: the MMAs reading
-        // the slot are done (both CTAs)
-        uint64_t afull[ASTAGES], aempty[ASTAGES], bfull[BSTAGES], bempty[BSTAGES], raw_full[RSTAGES],
-            raw_empty[RSTAGES], acc_full[2], acc_empty[2], drain;
+        // full: CTA 0 -- its A stage landed (its TMA), CTA 1's forward of its own, and both B
+        // halves built (4 local + 4 remote producer warps): 10 arrivals; CTA 1 -- its A stage
+        // landed (1). empty: the MMAs reading the slot are done (both CTAs, one commit)
+        uint64_t full[STAGES], empty[STAGES], raw_full[RSTAGES], raw_empty[RSTAGES], acc_full[2], acc_empty[2],
+            drain;
         uint64_t stall;  // never arrived at: the wait of the debug_stall test hook
         uint32_t tmem_base;
         int abort;
@@ -328,7 +334,7 @@ __device__ __forceinline__ void advance(uint32_t &slot, uint32_t &phase)
 template <class C>
 __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const __grid_constant__ MmaMaps maps)
 {
-    constexpr int ASTAGES = C::ASTAGES, BSTAGES = C::BSTAGES, RSTAGES = C::RSTAGES, EPW = C::EPW;
+    constexpr int STAGES = C::STAGES, RSTAGES = C::RSTAGES, EPW = C::EPW;
     using Smem = typename C::Smem;
     extern __shared__ uint8_t smem_raw[];
     // the operand stages need 1024-byte alignment (128-byte swizzle atoms); the offset is the
@@ -347,7 +353,7 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
     }
     // each CTA's B half holds six column types in rows 0-125: rows 126-127 stay zero
     constexpr int ZR = NH - TYH * TJ;
-    for (int w = threadIdx.x; w < BSTAGES * ZR * 8; w += blockDim.x) {
+    for (int w = threadIdx.x; w < STAGES * ZR * 8; w += blockDim.x) {
         const int st = w / (ZR * 8), n = TYH * TJ + (w / 8) % ZR, c = w % 8;
         *reinterpret_cast<uint4 *>(sm.b[st] + (n >> 3) * 1024 + (n & 7) * 128 + c * 16) = make_uint4(0, 0, 0, 0);
     }
@@ -361,13 +367,9 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
     unsigned int *const mxf = smax_local ? smax : a.maxf;
     unsigned int *const mxf2 = smax_local ? smax + a.ntraits : a.maxf2;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < ASTAGES; ++s) {
-            tc::mbar_init(&sm.afull[s], rank == 0 ? 2 : 1);
-            tc::mbar_init(&sm.aempty[s], 1);
-        }
-        for (int s = 0; s < BSTAGES; ++s) {
-            tc::mbar_init(&sm.bfull[s], rank == 0 ? 8 : 1);
-            tc::mbar_init(&sm.bempty[s], 1);
+        for (int s = 0; s < STAGES; ++s) {
+            tc::mbar_init(&sm.full[s], rank == 0 ? 10 : 1);
+            tc::mbar_init(&sm.empty[s], 1);
         }
         for (int r = 0; r < RSTAGES; ++r) {
             tc::mbar_init(&sm.raw_full[r], 1);
@@ -407,7 +409,7 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
             const Unit un = decode(a, u);
             if (un.skip) continue;
             for (int ks = 0; ks < nks; ++ks) {
-                if (!tc::mbar_wait(&sm.raw_full[rs], rph, abort, a.wait_ns) || !tc::mbar_wait(&sm.bempty[stage], phase ^ 1u, abort, a.wait_ns)) {
+                if (!tc::mbar_wait(&sm.raw_full[rs], rph, abort, a.wait_ns) || !tc::mbar_wait(&sm.empty[stage], phase ^ 1u, abort, a.wait_ns)) {
                     fail(a, sm, 2);
                     ok = false;
                     break;
@@ -464,10 +466,10 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                 __syncwarp();
                 if (lane == 0) {
                     tc::mbar_arrive(&sm.raw_empty[rs]);
-                    if (rank == 0) tc::mbar_arrive(&sm.bfull[stage]);
-                    else tc::mbar_arrive_remote(&sm.bfull[stage], 0);
+                    if (rank == 0) tc::mbar_arrive(&sm.full[stage]);
+                    else tc::mbar_arrive_remote(&sm.full[stage], 0);
                 }
-                advance<BSTAGES>(stage, phase);
+                advance<STAGES>(stage, phase);
                 advance<RSTAGES>(rs, rph);
             }
         }
@@ -693,17 +695,17 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                 if (un.skip) continue;
                 const int arow = 3 * (un.bd.start1 + un.i0 + TI * (int)rank);
                 for (int ks = 0; ks < nks; ++ks) {
-                    if (!tc::mbar_wait(&sm.aempty[as], aph ^ 1u, abort, a.wait_ns)) {
+                    if (!tc::mbar_wait(&sm.empty[as], aph ^ 1u, abort, a.wait_ns)) {
                         fail(a, sm, 7);
                         ok = false;
                         break;
                     }
-                    tc::mbar_arrive_expect_tx(&sm.afull[as], A_BYTES);
+                    tc::mbar_arrive_expect_tx(&sm.full[as], A_BYTES);
 #pragma unroll
                     for (int w = 0; w < 4; ++w)
-                        tc::tma_load_2d(sm.a[as] + 32 * w * KS, &maps.hi, ks * KS, arow + A_BOX * w, &sm.afull[as]);
+                        tc::tma_load_2d(sm.a[as] + 32 * w * KS, &maps.hi, ks * KS, arow + A_BOX * w, &sm.full[as]);
                     ++issued_a;
-                    advance<ASTAGES>(as, aph);
+                    advance<STAGES>(as, aph);
                 }
             }
             // no TMA write may still be landing in shared memory when the CTA exits: wait for
@@ -712,9 +714,9 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
             // through the phases it can observe (all its issued phases complete on the normal
             // path; after an abort the bounded wait ends).
             int no_abort = 0;
-            for (uint32_t back = 1; back <= ASTAGES && back <= issued_a; ++back) {
-                const uint32_t slot = (as + ASTAGES - back) % ASTAGES, par = back > as ? (aph ^ 1u) : aph;
-                if (!tc::mbar_wait(&sm.afull[slot], par, &no_abort, a.wait_ns)) fail(a, sm, 8);
+            for (uint32_t back = 1; back <= STAGES && back <= issued_a; ++back) {
+                const uint32_t slot = (as + STAGES - back) % STAGES, par = back > as ? (aph ^ 1u) : aph;
+                if (!tc::mbar_wait(&sm.full[slot], par, &no_abort, a.wait_ns)) fail(a, sm, 8);
             }
         }
     } else if (warp == 14) {
@@ -749,25 +751,25 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
         }
     } else if (warp == 12 && lane == 0 && rank == 1) {
         // ---------------- A forwarder (CTA 1, warp 12) ----------------
-        // each of this CTA's A stages, once landed, counts as one arrival on CTA 0's afull
+        // each of this CTA's A stages, once landed, counts as one arrival on CTA 0's full
         uint32_t as = 0, aph = 0;
         bool ok = true;
         for (long long u = pair; u < units && ok; u += npairs) {
             const Unit un = decode(a, u);
             if (un.skip) continue;
             for (int ks = 0; ks < nks; ++ks) {
-                if (!tc::mbar_wait(&sm.afull[as], aph, abort, a.wait_ns)) {
+                if (!tc::mbar_wait(&sm.full[as], aph, abort, a.wait_ns)) {
                     fail(a, sm, 9);
                     ok = false;
                     break;
                 }
-                tc::mbar_arrive_remote(&sm.afull[as], 0);
-                advance<ASTAGES>(as, aph);
+                tc::mbar_arrive_remote(&sm.full[as], 0);
+                advance<STAGES>(as, aph);
             }
         }
     } else if (warp == 12 && lane == 0) {
         // ---------------- MMA issuer (CTA 0, warp 12) ----------------
-        uint32_t as = 0, aph = 0, bs = 0, bph = 0, accph[2] = {0u, 0u};
+        uint32_t as = 0, aph = 0, accph[2] = {0u, 0u};
         int buf = 0;
         bool ok = true;
         // test hook: the first CTA pair's issuer waits on a barrier that nothing arrives at, so
@@ -786,22 +788,19 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
             tc::tc_fence_after();
             const uint32_t d = tmem + acc_col(buf);
             for (int ks = 0; ks < nks; ++ks) {
-                if (!tc::mbar_wait_cluster(&sm.bfull[bs], bph, abort, a.wait_ns) ||
-                    !tc::mbar_wait_cluster(&sm.afull[as], aph, abort, a.wait_ns)) {
+                if (!tc::mbar_wait_cluster(&sm.full[as], aph, abort, a.wait_ns)) {
                     fail(a, sm, 5);
                     ok = false;
                     break;
                 }
                 tc::tc_fence_after();
-                const uint32_t asb = tc::smem_u32(sm.a[as]), bsb = tc::smem_u32(sm.b[bs]);
+                const uint32_t asb = tc::smem_u32(sm.a[as]), bsb = tc::smem_u32(sm.b[as]);
 #pragma unroll
                 for (int kk = 0; kk < KS / 32; ++kk)
                     tc::mma_i8_pair(d, tc::smem_desc_sw128(asb + 32 * kk), tc::smem_desc_sw128(bsb + 32 * kk), IDESC,
                                     (ks | kk) != 0);
-                tc::mma_commit_pair_mc(&sm.aempty[as], 0x3);
-                tc::mma_commit_pair_mc(&sm.bempty[bs], 0x3);
-                advance<ASTAGES>(as, aph);
-                advance<BSTAGES>(bs, bph);
+                tc::mma_commit_pair_mc(&sm.empty[as], 0x3);
+                advance<STAGES>(as, aph);
             }
             if (!ok) break;
             tc::mma_commit_pair_mc(&sm.acc_full[buf], 0x3);
@@ -873,22 +872,23 @@ int mma_min_nid() { return 256; }
 int mma_max_nid() { return 1 << 24; }  // digit sums stay within int32
 int mma_stage_individuals() { return mma::KS; }
 
-// The variants the autotuner chooses among -- ring depths (A, B, raw stages; each fills the
-// SM's shared memory to about 200 KB) and epilogue warps per TMEM lane quarter:
-//   0  7 / 3 / 10, 2 epilogue warps   1  6 / 4 / 8, 2   2  8 / 3 / 6, 2   3  7 / 3 / 10, 3
-using Rings0 = mma::Rings<7, 3, 10>;
-using Rings1 = mma::Rings<6, 4, 8>;
-using Rings2 = mma::Rings<8, 3, 6>;
-using Rings3 = mma::Rings<7, 3, 10, 3>;
+// The variants the autotuner chooses among -- operand slots and raw stages (each ~200-216 KB
+// of shared memory) and epilogue warps per TMEM lane quarter:
+//   0  6 slots / 6 raw, 2 epilogue warps   1  5 / 10, 2   2  6 / 4, 2   3  6 / 6, 3
+using Rings0 = mma::Rings<6, 6>;
+using Rings1 = mma::Rings<5, 10>;
+using Rings2 = mma::Rings<6, 4>;
+using Rings3 = mma::Rings<6, 6, 3>;
 constexpr int MMA_SHAPES = 4;
 
 int mma_shapes() { return MMA_SHAPES; }
 
 void mma_shape(int v, const char **desc)
 {
-    static const char *names[MMA_SHAPES] = {"rings A7/B3/R10, 8 epilogue warps", "rings A6/B4/R8, 8 epilogue warps",
-                                            "rings A8/B3/R6, 8 epilogue warps",
-                                            "rings A7/B3/R10, 12 epilogue warps (setmaxnreg)"};
+    static const char *names[MMA_SHAPES] = {"6 operand slots / 6 raw stages, 8 epilogue warps",
+                                            "5 operand slots / 10 raw stages, 8 epilogue warps",
+                                            "6 operand slots / 4 raw stages, 8 epilogue warps",
+                                            "6 operand slots / 6 raw stages, 12 epilogue warps (setmaxnreg)"};
     if (desc) *desc = names[v];
 }
 
