@@ -109,18 +109,23 @@ static_assert(bcol(NTYPE - 1, 3 * (ROUNDS - 1)) + 3 < N && bcol(TYH - 1, 3 * (RO
 // wait and one commit: the issuer is the pipeline's critical path (a barrier wait costs about a
 // hundred cycles even when the barrier is ready).
 //
-// EPW epilogue warps per TMEM lane quarter: 2 (15 warps: epilogue 0-3 and 8-11) or 3 (20 warps:
-// epilogue also 16-19, warp 15 idle). With 3, the 640 threads launch with 96 registers each
-// and the warpgroups rebalance (setmaxnreg): the three epilogue warpgroups to 128, the B
-// producers to 56, the loaders and MMA issuer to 40 -- 3 x 128 x 128 + 128 x 56 + 128 x 40
-// = 61,440 = 640 x 96, the launch's pool.
-template <int S, int RSx, int EPW_ = 2>
+// EPW epilogue warps per TMEM lane quarter: 2 (epilogue warps 0-3 and 8-11) or 3 (also 16-19).
+// PW producer groups of 4 warps: 1 (warps 4-7) or 2 (also 16-19, the groups taking alternate
+// stages, so each has two stage times for its loads, stores, proxy fence and arrivals: the
+// producers' per-stage latency, not their throughput, bounds the pipeline). One group and two
+// epilogue warps: 15 warps. Otherwise 20 warps (warp 15 idle), launched with 96 registers each
+// and rebalanced by warpgroup (setmaxnreg): epilogue warpgroups to 128, producer warpgroups to
+// 56 (EPW 3) or 88 (PW 2), the loaders and MMA issuer to 40 -- 3 x 128 x 128 + 128 x 56 +
+// 128 x 40 = 61,440 and 2 x 128 x 128 + 2 x 128 x 88 + 128 x 40 = 60,416, within the launch's
+// pool of 640 x 96 = 61,440.
+template <int S, int RSx, int EPW_ = 2, int PW_ = 1>
 struct Rings {
-    static constexpr int STAGES = S, RSTAGES = RSx, EPW = EPW_;
-    static constexpr int NWARPS = EPW == 2 ? 15 : 20;
+    static constexpr int STAGES = S, RSTAGES = RSx, EPW = EPW_, PW = PW_;
+    static constexpr int NWARPS = (EPW == 2 && PW == 1) ? 15 : 20;
     static constexpr int NTHREADS = NWARPS * 32;
-    static_assert(EPW == 2 || EPW == 3, "epilogue warps per lane quarter");
-    static_assert(EPW == 2 || 3 * 128 * 128 + 128 * 56 + 128 * 40 == NTHREADS * 96, "register split");
+    static constexpr int PROD_REGS = PW == 2 ? 88 : 56;
+    static_assert((EPW == 2 || EPW == 3) && (PW == 1 || PW == 2) && !(EPW == 3 && PW == 2), "warp roles");
+    static_assert(NWARPS == 15 || EPW * 128 * 128 + PW * 128 * PROD_REGS + 128 * 40 <= NTHREADS * 96, "register split");
     struct Smem {
         uint8_t a[STAGES][A_STAGE];
         uint8_t b[STAGES][B_STAGE];
@@ -334,7 +339,7 @@ __device__ __forceinline__ void advance(uint32_t &slot, uint32_t &phase)
 template <class C>
 __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const __grid_constant__ MmaMaps maps)
 {
-    constexpr int STAGES = C::STAGES, RSTAGES = C::RSTAGES, EPW = C::EPW;
+    constexpr int STAGES = C::STAGES, RSTAGES = C::RSTAGES, EPW = C::EPW, PW = C::PW;
     using Smem = typename C::Smem;
     extern __shared__ uint8_t smem_raw[];
     // the operand stages need 1024-byte alignment (128-byte swizzle atoms); the offset is the
@@ -391,24 +396,34 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
     const uint32_t tmem = sm.tmem_base;
     volatile int *abort = &sm.abort;
 
-    // epilogue warps: 0-3, 8-11 (and 16-19 with three per lane quarter)
-    const bool epi_warp = warp < 4 || (warp >= 8 && warp < 12) || warp >= 16;
-    if constexpr (EPW == 3) {
+    // epilogue warps: 0-3, 8-11 (and 16-19 with three per lane quarter); producer warps: 4-7
+    // (and 16-19 with two producer groups)
+    const bool epi_warp = warp < 4 || (warp >= 8 && warp < 12) || (EPW == 3 && warp >= 16);
+    const bool prod_warp = (warp >= 4 && warp < 8) || (PW == 2 && warp >= 16);
+    if constexpr (C::NWARPS == 20) {
         if (epi_warp) tc::setmaxnreg_inc<128>();
-        else if (warp >= 4 && warp < 8) tc::setmaxnreg_dec<56>();
+        else if (prod_warp) tc::setmaxnreg_dec<C::PROD_REGS>();
         else tc::setmaxnreg_dec<40>();
     }
-    if (warp >= 4 && warp < 8) {
+    if (prod_warp) {
         // ---------------- B producers: thread -> (j-SNP, 16-individual chunk) ----------------
-        // items (jj, c) with jj < 16 for every thread, and (16 + t/8, c) for t < XTRA
-        const int t = threadIdx.x - 128, jj = t >> 3, c = t & 7;
+        // items (jj, c) with jj < 16 for every thread, and (16 + t/8, c) for t < XTRA; with two
+        // groups, group pg builds the stages whose sequence number is pg modulo 2 (and follows
+        // the ring positions of the others without touching them)
+        const int pg = warp >= 16 ? 1 : 0;
+        const int t = threadIdx.x - (pg ? 512 : 128), jj = t >> 3, c = t & 7;
         const bool xtra = t < XTRA;
-        uint32_t stage = 0, phase = 0, rs = 0, rph = 0;
+        uint32_t stage = 0, phase = 0, rs = 0, rph = 0, seq = 0;
         bool ok = true;
         for (long long u = pair; u < units && ok; u += npairs) {
             const Unit un = decode(a, u);
             if (un.skip) continue;
             for (int ks = 0; ks < nks; ++ks) {
+                if ((int)(seq++ % (uint32_t)PW) != pg) {
+                    advance<STAGES>(stage, phase);
+                    advance<RSTAGES>(rs, rph);
+                    continue;
+                }
                 if (!tc::mbar_wait(&sm.raw_full[rs], rph, abort, a.wait_ns) || !tc::mbar_wait(&sm.empty[stage], phase ^ 1u, abort, a.wait_ns)) {
                     fail(a, sm, 2);
                     ok = false;
@@ -875,11 +890,13 @@ int mma_stage_individuals() { return mma::KS; }
 // The variants the autotuner chooses among -- operand slots and raw stages (each ~200-216 KB
 // of shared memory) and epilogue warps per TMEM lane quarter:
 //   0  6 slots / 6 raw, 2 epilogue warps   1  5 / 10, 2   2  6 / 4, 2   3  6 / 6, 3
+//   4  6 / 6, 2 epilogue warps, two producer groups on alternate stages
 using Rings0 = mma::Rings<6, 6>;
 using Rings1 = mma::Rings<5, 10>;
 using Rings2 = mma::Rings<6, 4>;
 using Rings3 = mma::Rings<6, 6, 3>;
-constexpr int MMA_SHAPES = 4;
+using Rings4 = mma::Rings<6, 6, 2, 2>;
+constexpr int MMA_SHAPES = 5;
 
 int mma_shapes() { return MMA_SHAPES; }
 
@@ -888,7 +905,8 @@ void mma_shape(int v, const char **desc)
     static const char *names[MMA_SHAPES] = {"6 operand slots / 6 raw stages, 8 epilogue warps",
                                             "5 operand slots / 10 raw stages, 8 epilogue warps",
                                             "6 operand slots / 4 raw stages, 8 epilogue warps",
-                                            "6 operand slots / 6 raw stages, 12 epilogue warps (setmaxnreg)"};
+                                            "6 operand slots / 6 raw stages, 12 epilogue warps (setmaxnreg)",
+                                            "6 operand slots / 6 raw stages, 8 epilogue warps, 2 producer groups (setmaxnreg)"};
     if (desc) *desc = names[v];
 }
 
@@ -972,6 +990,7 @@ cudaError_t mma_prepare(int v, int ntraits, int grid_request, int *grid)
     case 1: return prepare<Rings1>(v, ntraits, grid_request, grid);
     case 2: return prepare<Rings2>(v, ntraits, grid_request, grid);
     case 3: return prepare<Rings3>(v, ntraits, grid_request, grid);
+    case 4: return prepare<Rings4>(v, ntraits, grid_request, grid);
     }
     return cudaErrorInvalidValue;
 }
@@ -984,6 +1003,7 @@ cudaError_t mma_enqueue(int v, const ScanArgs &a, const MmaMaps &maps, int grid,
     case 1: return enqueue<Rings1>(a, maps, grid, stream);
     case 2: return enqueue<Rings2>(a, maps, grid, stream);
     case 3: return enqueue<Rings3>(a, maps, grid, stream);
+    case 4: return enqueue<Rings4>(a, maps, grid, stream);
     }
     return cudaErrorInvalidValue;
 }
