@@ -8,8 +8,9 @@
 //   A rows (row 32w + l, l < 30): i-SNP 10w + l/3, genotype a = l%3: [g_i(k) == a]
 //   B cols: type t = 4b + s (b = 0..2 the j genotype, s = 0..3), [g_j(k) == b] * D_s(k), with
 //     D_0 = w_k (phenotype valid) and D_1..3 the balanced base-256 digits of the fixed-point
-//     phenotype Y_k = round(y_k * 2^sy) (y centred, 0 when invalid); column of (t, j') in
-//     the pair MMA: 128 (t / 6) + 21 (t % 6) + j' (each CTA of the pair holds six types).
+//     phenotype Y_k = round(y_k * 2^sy) (y centred, 0 when invalid); CTA 0 of the pair holds
+//     the types of D_0 and D_1, CTA 1 those of D_2 and D_3, so each builds its half from two
+//     digit rows: column of (t, j') in the pair MMA 128 (s / 2) + 21 (2b + s % 2) + j'.
 // int8 operands, int32 accumulation: counts and digit sums are exact, so
 //     S_ab = (D1 + 256 D2 + 65536 D3) * 2^-sy exactly for the quantised phenotype.
 // The sum of ytilde^2 (ytilde = Y 2^-sy) over the pair's valid individuals (both genotypes
@@ -38,7 +39,7 @@
 //   warp 14       raw loader (one thread): per stage, the j-tile's 21 one-hot rows and the
 //                 trait's 4 digit rows, up to RSTAGES stages ahead of the B producers
 //   warps 4-7     B producers: raw rows -> this CTA's half of the B stage (K-major, 128-byte
-//                 swizzle): CTA 0 column types 0-5, CTA 1 types 6-11
+//                 swizzle): CTA 0 the column types of digit rows 0-1, CTA 1 of rows 2-3
 //   warp 12       CTA 0: MMA issuer (one thread): 4 pair MMAs per stage; CTA 1: forwards the
 //                 completion of its own A stages to CTA 0. Both: TMEM allocation (pair form)
 //   warps 0-3, 8-11  epilogue, two warps per TMEM lane quarter, seven j rounds between them
@@ -77,8 +78,12 @@ constexpr int ND = 4;          // digit rows per trait: w, Y digits (3)
 constexpr int ROUNDS = (TJ + 2) / 3;  // j rounds of the epilogue (3 j-SNPs per round)
 constexpr uint32_t ACC_COL1 = N;
 __host__ __device__ constexpr uint32_t acc_col(uint32_t buf) { return buf ? ACC_COL1 : 0u; }
-// accumulator column of column type ty, j-SNP jj of the tile
-__host__ __device__ constexpr int bcol(int ty, int jj) { return (ty / TYH) * NH + (ty % TYH) * TJ + jj; }
+// accumulator column of column type ty = 4b + s, j-SNP jj of the tile: digit rows s = 0, 1 in
+// CTA 0's half, 2, 3 in CTA 1's, six types of 21 columns each
+__host__ __device__ constexpr int bcol(int ty, int jj)
+{
+    return ((ty & 3) >> 1) * NH + (2 * (ty >> 2) + (ty & 1)) * TJ + jj;
+}
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int A_STAGE = (M / 2) * KS;  // 16 KB
 constexpr int B_STAGE = NH * KS;       // 16 KB
@@ -95,12 +100,12 @@ constexpr int XTRA = TJ * 8 - 128;
 constexpr uint32_t IDESC = tc::idesc_i8(M, N);
 static_assert(RAW_D % 1024 == 0 && RAW_D + ND * KS <= RAW_STAGE, "raw layout");
 static_assert(B_STAGE % 1024 == 0 && A_STAGE % 1024 == 0 && N % 32 == 0 && N <= 256 && NCOL <= N, "operand tiles");
-static_assert(NTYPE % 2 == 0 && TYH * TJ <= NH && TYH == 6, "B split: CTA 0 types 0-5, CTA 1 types 6-11");
+static_assert(NTYPE % 2 == 0 && TYH * TJ <= NH && TYH == 6, "B split: six types per CTA");
 static_assert(XTRA >= 0 && XTRA <= 128 && (XTRA % 8) == 0 && 16 + XTRA / 8 == TJ, "producer items");
 static_assert(2 * N <= (int)TMEM_COLS, "TMEM layout: two accumulators");
 // the x4 accumulator loads of a round's three j-SNPs read one column past them: within the
 // pair's 256 columns even for the last type of each half
-static_assert(bcol(NTYPE - 1, 3 * (ROUNDS - 1)) + 3 < N && bcol(TYH - 1, 3 * (ROUNDS - 1)) + 3 < NH, "epilogue loads");
+static_assert(bcol(11, 3 * (ROUNDS - 1)) + 3 < N && bcol(9, 3 * (ROUNDS - 1)) + 3 < NH, "epilogue loads");
 
 // Ring depths (a kernel variant, chosen by the autotuner): STAGES operand slots, each an A stage
 // (TMA from L2 / DRAM) and a B stage (built from raw rows already in shared memory), and the raw
@@ -431,14 +436,13 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                 }
                 const uint8_t *raw = sm.raw[rs];
                 uint8_t *base = sm.b[stage];
-                uint4 d[ND];
-#pragma unroll
-                for (int s2 = 0; s2 < ND; ++s2) d[s2] = ld_sw128(raw + RAW_D, s2, c);
-                // column type ty (genotype ty / 4, digit row ty % 4) of j-SNP jx at local row
-                // (ty - 6 rank) * 21 + jx
-                auto put = [&](int ty, int jx, const uint4 &m) {
-                    const int n = (ty - TYH * (int)rank) * TJ + jx;
-                    const uint4 &dv = d[ty & 3];
+                // this CTA's two digit rows: 2 rank and 2 rank + 1
+                const uint4 d[2] = {ld_sw128(raw + RAW_D, 2 * (int)rank, c), ld_sw128(raw + RAW_D, 2 * (int)rank + 1, c)};
+                // local type q = 2b + s' (genotype b, this CTA's digit row s') of j-SNP jx at
+                // local row 21 q + jx
+                auto put = [&](int q, int jx, const uint4 &m) {
+                    const int n = q * TJ + jx;
+                    const uint4 &dv = d[q & 1];
                     uint4 o;
                     o.x = m.x & dv.x;
                     o.y = m.y & dv.y;
@@ -457,20 +461,11 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                 };
                 auto build = [&](int jx) {
                     const uint4 h = ld_sw128(raw + RAW_J, jx, c);
-                    if (rank == 0) {
-                        // types 0-5: genotype 0 x {w, d0, d1, d2}, genotype 1 x {w, d0}
-                        const uint4 m0 = gmask(h, 0), m1 = gmask(h, 1);
 #pragma unroll
-                        for (int ty = 0; ty < 4; ++ty) put(ty, jx, m0);
-                        put(4, jx, m1);
-                        put(5, jx, m1);
-                    } else {
-                        // types 6-11: genotype 1 x {d1, d2}, genotype 2 x {w, d0, d1, d2}
-                        const uint4 m1 = gmask(h, 1), m2 = gmask(h, 2);
-                        put(6, jx, m1);
-                        put(7, jx, m1);
-#pragma unroll
-                        for (int ty = 8; ty < 12; ++ty) put(ty, jx, m2);
+                    for (int b = 0; b < 3; ++b) {
+                        const uint4 m = gmask(h, b);
+                        put(2 * b, jx, m);
+                        put(2 * b + 1, jx, m);
                     }
                 };
                 build(jj);
