@@ -455,11 +455,11 @@ def main():
             ops_pair = 2.0 * 36.0 * nid
             achieved = pairs_launch * ops_pair / kern_s / 1e12
             # DRAM bytes per launch: the ncu capture of the same kernel on the cfg3m workload
-            # (N=10,000, M=20,000, operands larger than L2) read and wrote 18.02 GB for
+            # (N=10,000, M=20,000, operands larger than L2) read and wrote 16.89 GB for
             # 199,990,000 pairs over Np = 10,112 padded individuals; the j rows are streamed
             # once per i tile, so the bytes scale with pairs x Np
             np_pad = (nid + 127) // 128 * 128
-            traffic = 18.02e9 / (199990000.0 * 10112.0) * pairs_launch * np_pad
+            traffic = 16.89e9 / (199990000.0 * 10112.0) * pairs_launch * np_pad
             # the same against twice the measured dense bf16 rate (dense int8 runs at twice bf16)
             peaks2 = measured_peaks()[0]
             bf16x2 = 2.0 * peaks2["bf16_tflops"] if peaks2 and peaks2.get("bf16_tflops") else None
