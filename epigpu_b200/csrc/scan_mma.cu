@@ -33,13 +33,15 @@
 // A comes straight from HBM: the genotype-indicator rows h3 (row 3s + a = [g_s == a] bytes)
 // are TMA-loaded into a 128-byte-swizzled shared-memory stage and read by the MMA from there.
 //
-// Per CTA, 15 warps:
+// Per CTA, 15 warps (20 in the variants with three epilogue warps per lane quarter or two
+// producer groups; Rings below):
 //   warp 13       A loader (one thread): per 128-individual stage, the CTA's A stage (four
 //                 2-D tiled loads of 30 h3 rows into rows 32w..32w+29); no multicast
 //   warp 14       raw loader (one thread): per stage, the j-tile's 21 one-hot rows and the
 //                 trait's 4 digit rows, up to RSTAGES stages ahead of the B producers
 //   warps 4-7     B producers: raw rows -> this CTA's half of the B stage (K-major, 128-byte
-//                 swizzle): CTA 0 the column types of digit rows 0-1, CTA 1 of rows 2-3
+//                 swizzle): CTA 0 the column types of digit rows 0-1, CTA 1 of rows 2-3;
+//                 a second producer group (warps 16-19) takes alternate stages in one variant
 //   warp 12       CTA 0: MMA issuer (one thread): 4 pair MMAs per stage; CTA 1: forwards the
 //                 completion of its own A stages to CTA 0. Both: TMEM allocation (pair form)
 //   warps 0-3, 8-11  epilogue, two warps per TMEM lane quarter, seven j rounds between them
