@@ -745,10 +745,13 @@ epi_status pick_variant(epi_ctx *ctx, const epi_scan_opts *o, int form, int *v, 
         return EPI_OK;
     }
     // sample: an off-diagonal s x s block (every pair valid) when the genome holds one, with
-    // enough tiles for about four waves over the SMs at this trait count
+    // enough tiles for about sixteen waves over the SMs at this trait count, at least 1,024
+    // SNPs a side (a smaller block ranked the tensor variants wrongly at 64 traits) unless that
+    // makes more than 2^28 pair tests, and at most 2,048
     const int T = ctx->ntraits;
-    int s = (int)std::ceil(std::sqrt(4.0 * ctx->sm_count * 4096.0 / T));
-    s = std::max(256, std::min(s, 2048));
+    int s = (int)std::ceil(std::sqrt(16.0 * ctx->sm_count * 4096.0 / T));
+    const int lo = std::max(256, std::min(1024, (int)std::sqrt(268435456.0 / T)));
+    s = std::max(lo, std::min(s, 2048));
     epi_block blk;
     if (ctx->nsnp >= 2 * s) blk = {s, s, 0, s};
     else blk = {0, ctx->nsnp, 0, ctx->nsnp};
