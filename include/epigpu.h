@@ -77,8 +77,9 @@ typedef struct epi_scan_opts {
     int32_t no_graph;      /* 0: the scan's device work is captured as a CUDA graph and a repeat of
                             * the same scan shape (kernel arguments, blocks) replays it with one
                             * launch; 1: every operation is launched directly */
-    int32_t tile_config;   /* 0: the kernel variant (plain form: tile shape; tensor form: ring
-                            * depths) is chosen by the autotuner, which times every candidate
+    int32_t tile_config;   /* 0: the kernel variant (plain form: tile shape, 3 candidates;
+                            * tensor form: ring depths, epilogue warps and producer groups, 5
+                            * candidates) is chosen by the autotuner, which times every candidate
                             * on a sample block once per device, form, individual count and
                             * trait count; k >= 1: candidate k (epi_scan_config names it) */
     int32_t reserved[5];   /* set to 0 */
