@@ -10,7 +10,8 @@
 //     D_0 = w_k (phenotype valid) and D_1..3 the balanced base-256 digits of the fixed-point
 //     phenotype Y_k = round(y_k * 2^sy) (y centred, 0 when invalid); CTA 0 of the pair holds
 //     the types of D_0 and D_1, CTA 1 those of D_2 and D_3, so each builds its half from two
-//     digit rows: column of (t, j') in the pair MMA 128 (s / 2) + 21 (2b + s % 2) + j'.
+//     digit rows: column of (t, j') in the pair MMA 128 (s / 2) + 6 j' + (2b + s % 2), the six
+//     columns of a j-SNP side by side in each half.
 // int8 operands, int32 accumulation: counts and digit sums are exact, so
 //     S_ab = (D1 + 256 D2 + 65536 D3) * 2^-sy exactly for the quantised phenotype.
 // The sum of ytilde^2 (ytilde = Y 2^-sy) over the pair's valid individuals (both genotypes
@@ -81,11 +82,12 @@ constexpr int ROUNDS = (TJ + 2) / 3;  // j rounds of the epilogue (3 j-SNPs per 
 constexpr uint32_t ACC_COL1 = N;
 __host__ __device__ constexpr uint32_t acc_col(uint32_t buf) { return buf ? ACC_COL1 : 0u; }
 // accumulator column of column type ty = 4b + s, j-SNP jj of the tile: digit rows s = 0, 1 in
-// CTA 0's half, 2, 3 in CTA 1's, six types of 21 columns each
-__host__ __device__ constexpr int bcol(int ty, int jj)
-{
-    return ((ty & 3) >> 1) * NH + (2 * (ty >> 2) + (ty & 1)) * TJ + jj;
-}
+// CTA 0's half, 2, 3 in CTA 1's; in each half the six local types q = 2b + s % 2 of a j-SNP
+// are adjacent (column 6 jj + q)
+__host__ __device__ constexpr int bq(int ty) { return 2 * (ty >> 2) + (ty & 1); }
+__host__ __device__ constexpr int bcol(int ty, int jj) { return ((ty & 3) >> 1) * NH + 6 * jj + bq(ty); }
+// the epilogue loads a round's three j-SNPs as 20 adjacent columns per half (five x4 loads)
+constexpr int RCOLS = 20;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int A_STAGE = (M / 2) * KS;  // 16 KB
 constexpr int B_STAGE = NH * KS;       // 16 KB
@@ -105,9 +107,9 @@ static_assert(B_STAGE % 1024 == 0 && A_STAGE % 1024 == 0 && N % 32 == 0 && N <= 
 static_assert(NTYPE % 2 == 0 && TYH * TJ <= NH && TYH == 6, "B split: six types per CTA");
 static_assert(XTRA >= 0 && XTRA <= 128 && (XTRA % 8) == 0 && 16 + XTRA / 8 == TJ, "producer items");
 static_assert(2 * N <= (int)TMEM_COLS, "TMEM layout: two accumulators");
-// the x4 accumulator loads of a round's three j-SNPs read one column past them: within the
-// pair's 256 columns even for the last type of each half
-static_assert(bcol(11, 3 * (ROUNDS - 1)) + 3 < N && bcol(9, 3 * (ROUNDS - 1)) + 3 < NH, "epilogue loads");
+// the accumulator loads of a round's three j-SNPs (18 columns per half) read two columns past
+// them: within each half even for the last round
+static_assert(6 * 3 * (ROUNDS - 1) + RCOLS <= NH && bcol(11, TJ - 1) < N && bcol(9, TJ - 1) < NH, "epilogue loads");
 
 // Ring depths (a kernel variant, chosen by the autotuner): STAGES operand slots, each an A stage
 // (TMA from L2 / DRAM) and a B stage (built from raw rows already in shared memory), and the raw
@@ -181,7 +183,7 @@ __device__ __forceinline__ void fail(const ScanArgs &a, Smem &sm, int where)
     if (atomicCAS(&a.counters[2], 0ull, 1ull) == 0ull) a.counters[3] = (unsigned long long)where;
 }
 
-__device__ __forceinline__ uint32_t sel3(const uint32_t v[4], int idx)
+__device__ __forceinline__ uint32_t sel3(const uint32_t v[3], int idx)
 {
     return idx == 0 ? v[0] : (idx == 1 ? v[1] : v[2]);
 }
@@ -441,9 +443,9 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                 // this CTA's two digit rows: 2 rank and 2 rank + 1
                 const uint4 d[2] = {ld_sw128(raw + RAW_D, 2 * (int)rank, c), ld_sw128(raw + RAW_D, 2 * (int)rank + 1, c)};
                 // local type q = 2b + s' (genotype b, this CTA's digit row s') of j-SNP jx at
-                // local row 21 q + jx
+                // local row 6 jx + q
                 auto put = [&](int q, int jx, const uint4 &m) {
-                    const int n = q * TJ + jx;
+                    const int n = 6 * jx + q;
                     const uint4 &dv = d[q & 1];
                     uint4 o;
                     o.x = m.x & dv.x;
@@ -535,11 +537,22 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                 const int gj = un.bd.start2 + (valid ? dj : 0);
                 const size_t mj = (size_t)t * a.nsnp + gj;
                 const double qmj = valid ? a.qm[mj] : 0.0;
-                uint32_t v[NTYPE][4];
+                // the round's columns of both halves, then v[ty][c] = type ty of j-SNP jb + c
+                uint32_t wv[2][RCOLS], v[NTYPE][3];
+                auto load_round = [&]() {
 #pragma unroll
-                for (int ty = 0; ty < NTYPE; ++ty)
-                    tc::tmem_ld4(acc + bcol(ty, jb), v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
-                tc::tmem_wait_ld();
+                    for (int h = 0; h < 2; ++h)
+#pragma unroll
+                        for (int k = 0; k < RCOLS / 4; ++k)
+                            tc::tmem_ld4(acc + h * NH + 6 * jb + 4 * k, wv[h][4 * k], wv[h][4 * k + 1], wv[h][4 * k + 2],
+                                         wv[h][4 * k + 3]);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int ty = 0; ty < NTYPE; ++ty)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) v[ty][c] = wv[(ty & 3) >> 1][6 * c + bq(ty)];
+                };
+                load_round();
                 // this lane's accumulator row (SNP i, genotype ga) folded per column c of the round
                 // (j-SNP jb + c): three counts and three FP32 phenotype sums. Up to 131,072
                 // individuals every digit sum is below 2^24 in magnitude, so the conversions are
@@ -605,10 +618,7 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                     // rare (pairs near a threshold or a running maximum, count dumps, small
                     // blocks): the exact digit sums of every cell, gathered again from the
                     // accumulator (still in TMEM until this warp releases it)
-#pragma unroll
-                    for (int ty = 0; ty < NTYPE; ++ty)
-                        tc::tmem_ld4(acc + bcol(ty, jb), v[ty][0], v[ty][1], v[ty][2], v[ty][3]);
-                    tc::tmem_wait_ld();
+                    load_round();
                     uint32_t r1[NTYPE], r2[NTYPE];
 #pragma unroll
                     for (int ty = 0; ty < NTYPE; ++ty) {
