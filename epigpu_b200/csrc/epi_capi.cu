@@ -47,6 +47,10 @@ cudaError_t mma_prepare(int v, int ntraits, int grid_request, int *grid);
 cudaError_t mma_enqueue(int v, const ScanArgs &a, const MmaMaps &maps, int grid, cudaStream_t stream);
 cudaError_t mma_encode_genotypes(MmaMaps *maps, const uint8_t *hcodes, const uint8_t *h3, int nsnp, int Np);
 cudaError_t mma_encode_traits(MmaMaps *maps, const int8_t *ydig, int ntraits, int Np);
+cudaError_t mma_encode_x(MmaMaps *maps, const int8_t *x, int nsnp, int Np, int ntraits);
+bool mma_needs_x(int v);
+cudaError_t launch_expand(const uint8_t *hcodes, const int8_t *ydig, int nsnp, int Np, int ntraits, int8_t *x,
+                          cudaStream_t stream);
 // Start of a scan: counters (hits, tile queue, error flag and site) to zero, the per-trait
 // maxima of F and F2 to the order-encoded -inf.
 __global__ void k_scan_init(unsigned long long *counters, unsigned int *maxf, int n)
@@ -86,6 +90,11 @@ struct epi_ctx {
            yscale_cap = 0;
     bool qm_valid = false;
     epi::MmaMaps maps;
+    // tensor form, streamed-B variant: the expanded B rows of every SNP and trait (12 bytes per
+    // SNP, individual and trait), built on first use after each genotype or trait load
+    int8_t *d_x = nullptr;
+    size_t x_cap = 0;
+    bool x_valid = false;
     std::vector<double> qc;
     // plain form: marginals per (trait, SNP) and the sum of y^2 per trait
     double *d_pmC = nullptr, *d_pmQ = nullptr, *d_ysq = nullptr;
@@ -221,7 +230,7 @@ epi_status epi_close(epi_ctx *ctx)
     void *bufs[] = {ctx->d_raw, ctx->d_planes, ctx->d_hcodes, ctx->d_h3, ctx->d_missbits, ctx->d_y, ctx->d_q,
                     ctx->d_wmask, ctx->d_qc, ctx->d_yscale, ctx->d_qd, ctx->d_qtot, ctx->d_qm, ctx->d_ydig,
                     ctx->d_hits, ctx->d_counters, ctx->d_maxf, ctx->d_blocks, ctx->d_maj, ctx->d_pmC,
-                    ctx->d_pmQ, ctx->d_ysq, ctx->d_pmN};
+                    ctx->d_pmQ, ctx->d_ysq, ctx->d_pmN, ctx->d_x};
     for (void *p : bufs)
         if (p) cudaFree(p);
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
@@ -268,6 +277,7 @@ epi_status epi_load_packed(epi_ctx *ctx, const int32_t *gpack, int32_t nid, int3
     CK(epi::launch_major(ctx->d_planes, nsnp, Wp, ctx->d_maj, ctx->stream));
     ctx->qm_valid = false;
     ctx->pm_valid = false;
+    ctx->x_valid = false;
     CK(epi::mma_encode_genotypes(&ctx->maps, ctx->d_hcodes, ctx->d_h3, nsnp, 32 * Wp));
     if (ctx->traits_nid != nid) ctx->ntraits = 0;  // traits no longer match
     ctx->nid = nid;
@@ -410,6 +420,7 @@ epi_status epi_set_traits(epi_ctx *ctx, const float *y, int32_t nid, int32_t ntr
     ctx->traits_nid = nid;
     ctx->qm_valid = false;
     ctx->pm_valid = false;
+    ctx->x_valid = false;
     return EPI_OK;
 }
 
@@ -483,6 +494,26 @@ int pick_form(const epi_ctx *ctx, const epi_scan_opts *o)
 }
 
 // Builds the kernel arguments and tile schedule for `blocks` and uploads the schedule.
+// Bytes of the streamed-B variant's expanded rows, and whether they may be allocated: at most
+// 32 GiB and half the device's free memory (beyond, that variant is not a candidate).
+static size_t x_bytes(const epi_ctx *ctx) { return 12 * (size_t)ctx->nsnp * ctx->Np * ctx->ntraits; }
+static bool x_usable(const epi_ctx *ctx)
+{
+    const size_t need = x_bytes(ctx);
+    if (need <= ctx->x_cap) return true;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return false;
+    return need <= (32ull << 30) && need <= fr / 2 + ctx->x_cap;
+}
+
+// The streamed-B variant as an autotuner candidate: only up to 6,144 padded individuals. Its
+// expanded rows are 12 bytes per SNP and individual, and the DRAM traffic of its super-tiles
+// grows with N per second of scanning; at N = 10,000 a full scan then runs into the 1 kW power
+// cap (SM clock ~1,350 MHz against ~1,935 MHz for the shared-memory producers) and ends 12%
+// slower, although the autotuner's short sample, run before the cap bites, ranks it 15% faster.
+// At N = 4,000 it is 10-14% faster at full clock. tile_config can still force it.
+static bool x_candidate(const epi_ctx *ctx) { return ctx->Np <= 6144 && x_usable(ctx); }
+
 epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const epi_scan_opts *o, ScanRun &r,
                      int variant)
 {
@@ -495,6 +526,18 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     if (r.form == EPI_FORM_POPC && ctx->nid > 65535)
         return set_err(ctx, EPI_E_UNSUPPORTED, "popcount form counts in 16 bits: at most 65535 individuals "
                        "(the reference's unsigned short counts, EpiOpenCL.c:68)");
+    if (r.form == EPI_FORM_TENSOR && epi::mma_needs_x(variant)) {
+        if (!x_usable(ctx))
+            return set_err(ctx, EPI_E_UNSUPPORTED, "tensor variant %d: its %zu bytes of expanded B rows do not fit",
+                           variant + 1, x_bytes(ctx));
+        if (!ctx->x_valid) {
+            CK(ensure(&ctx->d_x, &ctx->x_cap, x_bytes(ctx)));
+            CK(epi::launch_expand(ctx->d_hcodes, ctx->d_ydig, ctx->nsnp, ctx->Np, ctx->ntraits, ctx->d_x,
+                                  ctx->stream));
+            CK(epi::mma_encode_x(&ctx->maps, ctx->d_x, ctx->nsnp, ctx->Np, ctx->ntraits));
+            ctx->x_valid = true;
+        }
+    }
     int TI = epi::mma_tile_i(), TJ = epi::mma_tile_j();
     if (r.form == EPI_FORM_POPC) {
         epi::popc_shape(variant, &TI, &TJ, nullptr);
@@ -598,6 +641,12 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     a.t2 = o->t2;
     a.wait_ns = o->wait_limit_ms > 0 ? (unsigned long long)o->wait_limit_ms * 1000000ull : 2000000000ull;
     a.debug_stall = o->debug == EPI_DEBUG_STALL;
+    // streamed-B variant: super-tiles of about 40 MB of A rows (3 bytes per SNP and individual)
+    // and expanded B rows (12 per SNP, individual and trait), equal sides in pair tiles
+    {
+        const double per = (3.0 * epi::mma_tile_i() + 12.0 * epi::mma_tile_j() * ctx->ntraits) * ctx->Np;
+        a.xsi = a.xsj = std::max(1, (int)(40e6 / per));
+    }
     a.counters = ctx->d_counters;
     a.maxf = ctx->d_maxf;
     a.maxf2 = ctx->d_maxf + ctx->ntraits;
@@ -764,6 +813,12 @@ epi_status pick_variant(epi_ctx *ctx, const epi_scan_opts *o, int form, int *v, 
     o2.report_trait = 0;
     std::vector<float> ms(nv, 0.0f);
     for (int c = 0; c < nv; ++c) {
+        // the streamed-B variant is no candidate where its expanded rows would not fit or would
+        // run into the power cap (x_candidate)
+        if (form == EPI_FORM_TENSOR && epi::mma_needs_x(c) && !x_candidate(ctx)) {
+            ms[c] = INFINITY;
+            continue;
+        }
         ScanRun r;
         epi_status st = setup_run(ctx, &blk, 1, &o2, r, c);
         if (st != EPI_OK) return st;
@@ -783,7 +838,8 @@ epi_status pick_variant(epi_ctx *ctx, const epi_scan_opts *o, int form, int *v, 
     char buf[256];
     int len = snprintf(buf, sizeof(buf), "autotuned on a %d x %d-SNP block:", blk.size1, blk.size2);
     for (int c = 0; c < nv && len < (int)sizeof(buf); ++c)
-        len += snprintf(buf + len, sizeof(buf) - len, "%s %.3f ms", c ? " /" : "", ms[c]);
+        len += std::isfinite(ms[c]) ? snprintf(buf + len, sizeof(buf) - len, "%s %.3f ms", c ? " /" : "", ms[c])
+                                    : snprintf(buf + len, sizeof(buf) - len, "%s n/a", c ? " /" : "");
     *v = best;
     *how = buf;
     std::lock_guard<std::mutex> lock(g_tune_mu);

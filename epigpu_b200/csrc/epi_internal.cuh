@@ -95,6 +95,9 @@ struct ScanArgs {
     // tensor form: limit of every device-side wait (ns); test hook that makes one wait run out
     unsigned long long wait_ns;
     int32_t debug_stall;
+    // tensor form, streamed-B variant: the unit order walks super-tiles of xsi x xsj pair
+    // tiles, so that their A rows and expanded B rows stay in L2 together
+    int32_t xsi, xsj;
     // outputs
     DevHit *hits;
     int64_t cap;
@@ -114,7 +117,7 @@ struct ScanArgs {
 
 // TMA descriptors of the tensor form (kernel parameter, __grid_constant__)
 struct MmaMaps {
-    CUtensorMap hi, hj, dg;
+    CUtensorMap hi, hj, dg, hx;  // hx: the expanded B rows of the streamed-B variant
 };
 
 // TMA descriptors of the plain form: the genotype plane words, in boxes of the tile's i-SNPs

@@ -97,6 +97,37 @@ __global__ void k_qmiss(const uint32_t *__restrict__ missbits, int nsnp, int Wp,
     nm[gid] = (double)cnt;
 }
 
+// The streamed-B variant's expanded B rows: for trait t, CTA half h, SNP s and local column
+// type q = 2b + r (genotype b, digit row 2h + r of the trait: w, d0 for h = 0, d1, d2 for h = 1)
+// row ((t 2 + h) nsnp + s) 6 + q holds [g_s(k) == b] * digit(k) for every individual k -- the
+// rows the tensor form's producers otherwise build in shared memory. One thread per 16
+// individuals of (t, h, s).
+__global__ void k_expand(const uint8_t *__restrict__ hcodes, const int8_t *__restrict__ ydig, int nsnp, int Np,
+                         int ntraits, int8_t *__restrict__ x)
+{
+    const int nc = Np / 16;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)ntraits * 2 * nsnp * nc) return;
+    const int c = (int)(gid % nc);
+    const long long rest = gid / nc;
+    const int s = (int)(rest % nsnp);
+    const int h = (int)((rest / nsnp) % 2), t = (int)(rest / nsnp / 2);
+    const uint4 hc = reinterpret_cast<const uint4 *>(hcodes + (size_t)s * Np)[c];
+    const uint4 d0 = reinterpret_cast<const uint4 *>(ydig + ((size_t)t * 4 + 2 * h) * Np)[c];
+    const uint4 d1 = reinterpret_cast<const uint4 *>(ydig + ((size_t)t * 4 + 2 * h + 1) * Np)[c];
+    uint4 *out = reinterpret_cast<uint4 *>(x + (((size_t)t * 2 + h) * nsnp + s) * 6 * (size_t)Np) + c;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        uint4 m;
+        m.x = ((hc.x >> b) & 0x01010101u) * 0xFFu;
+        m.y = ((hc.y >> b) & 0x01010101u) * 0xFFu;
+        m.z = ((hc.z >> b) & 0x01010101u) * 0xFFu;
+        m.w = ((hc.w >> b) & 0x01010101u) * 0xFFu;
+        out[(size_t)(2 * b) * nc] = make_uint4(m.x & d0.x, m.y & d0.y, m.z & d0.z, m.w & d0.w);
+        out[(size_t)(2 * b + 1) * nc] = make_uint4(m.x & d1.x, m.y & d1.y, m.z & d1.z, m.w & d1.w);
+    }
+}
+
 // Per SNP the most frequent genotype (ties to the lower code), one warp per SNP: the plain
 // form derives that genotype's row of the 3x3 table from the SNP's marginals.
 __global__ void k_major(const uint4 *__restrict__ planes, int nsnp, int Wp, uint8_t *__restrict__ maj)
@@ -213,6 +244,15 @@ cudaError_t launch_qmiss(const uint32_t *missbits, int nsnp, int Wp, const uint3
     const int nt = 256;
     k_qmiss<<<(unsigned)((total + nt - 1) / nt), nt, 0, stream>>>(missbits, nsnp, Wp, wmask, qd, qr, Np, ntraits, qm,
                                                                      rm, nm);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_expand(const uint8_t *hcodes, const int8_t *ydig, int nsnp, int Np, int ntraits, int8_t *x,
+                          cudaStream_t stream)
+{
+    const long long total = (long long)ntraits * 2 * nsnp * (Np / 16);
+    const int nt = 256;
+    k_expand<<<(unsigned)((total + nt - 1) / nt), nt, 0, stream>>>(hcodes, ydig, nsnp, Np, ntraits, x);
     return cudaGetLastError();
 }
 

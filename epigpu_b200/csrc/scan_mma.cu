@@ -93,6 +93,7 @@ constexpr int A_STAGE = (M / 2) * KS;  // 16 KB
 constexpr int B_STAGE = NH * KS;       // 16 KB
 constexpr int A_BOX = 30;              // h3 rows per TMA box (10 i-SNPs x 3 genotypes)
 constexpr uint32_t A_BYTES = 4 * A_BOX * KS;  // transaction bytes per A stage (one CTA)
+constexpr uint32_t XB_BYTES = 6 * TJ * KS;     // the streamed-B variant: one CTA's B half (126 rows)
 // raw stage: the j-tile's one-hot rows and the trait's digit rows, 1024-aligned sections
 constexpr int RAW_J = 0, RAW_D = (TJ * KS + 1023) / 1024 * 1024;
 constexpr int RAW_STAGE = 4 * 1024;
@@ -127,9 +128,17 @@ static_assert(6 * 3 * (ROUNDS - 1) + RCOLS <= NH && bcol(11, TJ - 1) < N && bcol
 // 56 (EPW 3) or 88 (PW 2), the loaders and MMA issuer to 40 -- 3 x 128 x 128 + 128 x 56 +
 // 128 x 40 = 61,440 and 2 x 128 x 128 + 2 x 128 x 88 + 128 x 40 = 60,416, within the launch's
 // pool of 640 x 96 = 61,440.
-template <int S, int RSx, int EPW_ = 2, int PW_ = 1>
+//
+// XF (the streamed-B variant, single traits and sizes whose expanded B rows fit in HBM): B is
+// not built in shared memory but precomputed once per genotype and trait load into HBM (12
+// bytes per SNP and individual: `hx`, rows ((t 2 + half) M + snp) 6 + q) and TMA-loaded with
+// the A rows, one 126-row box per CTA half per stage; no producers or raw loader run (warps 4-7
+// and 14 idle) and CTA 0's full barrier counts two arrivals (its loader, CTA 1's forward).
+template <int S, int RSx, int EPW_ = 2, int PW_ = 1, bool XF_ = false>
 struct Rings {
     static constexpr int STAGES = S, RSTAGES = RSx, EPW = EPW_, PW = PW_;
+    static constexpr bool XF = XF_;
+    static_assert(!XF || (EPW == 2 && PW == 1), "the streamed-B variant runs the 15-warp layout");
     static constexpr int NWARPS = (EPW == 2 && PW == 1) ? 15 : 20;
     static constexpr int NTHREADS = NWARPS * 32;
     static constexpr int PROD_REGS = PW == 2 ? 88 : 56;
@@ -162,6 +171,11 @@ struct Unit {
     bool skip;
 };
 
+// Unit u -> (trait, block, pair tile). Units run trait-fastest over the block's tiles. XF (the
+// streamed-B variant): a block's tiles are walked in groups of xsi i-tiles, and within a group
+// in chunks of xsj j-tiles, i-tile by i-tile inside a chunk, so the clusters working at the same
+// time share a super-tile's A rows and expanded B rows in L2; otherwise i-tile by i-tile.
+template <bool XF = false>
 __device__ __forceinline__ Unit decode(const ScanArgs &a, long long u)
 {
     Unit r;
@@ -170,8 +184,23 @@ __device__ __forceinline__ Unit decode(const ScanArgs &a, long long u)
     r.block = find_block(a.blocks, a.nblocks, tile);
     r.bd = a.blocks[r.block];
     const long long lt = tile - r.bd.tile_base;
-    r.i0 = (int)(lt / r.bd.tiles_j) * TIP;  // the pair tile's first i-SNP
-    r.j0 = (int)(lt % r.bd.tiles_j) * TJ;
+    int ti, tj;
+    if (XF) {
+        const long long grp_tiles = (long long)a.xsi * r.bd.tiles_j;
+        const int grp = (int)(lt / grp_tiles);
+        const int ni = min(a.xsi, r.bd.tiles_i - grp * a.xsi);
+        const long long q = lt - (long long)grp * grp_tiles;
+        const int jc = (int)(q / ((long long)ni * a.xsj));
+        const int q2 = (int)(q - (long long)jc * ni * a.xsj);
+        const int nj = min(a.xsj, r.bd.tiles_j - jc * a.xsj);
+        ti = grp * a.xsi + q2 / nj;
+        tj = jc * a.xsj + q2 % nj;
+    } else {
+        ti = (int)(lt / r.bd.tiles_j);
+        tj = (int)(lt % r.bd.tiles_j);
+    }
+    r.i0 = ti * TIP;  // the pair tile's first i-SNP
+    r.j0 = tj * TJ;
     r.skip = r.bd.start1 + min(r.i0 + TIP, r.bd.size1) - 1 <= r.bd.start2 + r.j0;
     return r;
 }
@@ -382,7 +411,7 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
     unsigned int *const mxf2 = smax_local ? smax + a.ntraits : a.maxf2;
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
-            tc::mbar_init(&sm.full[s], rank == 0 ? 10 : 1);
+            tc::mbar_init(&sm.full[s], rank == 0 ? (C::XF ? 2 : 10) : 1);
             tc::mbar_init(&sm.empty[s], 1);
         }
         for (int r = 0; r < RSTAGES; ++r) {
@@ -408,7 +437,7 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
     // epilogue warps: 0-3, 8-11 (and 16-19 with three per lane quarter); producer warps: 4-7
     // (and 16-19 with two producer groups)
     const bool epi_warp = warp < 4 || (warp >= 8 && warp < 12) || (EPW == 3 && warp >= 16);
-    const bool prod_warp = (warp >= 4 && warp < 8) || (PW == 2 && warp >= 16);
+    const bool prod_warp = !C::XF && ((warp >= 4 && warp < 8) || (PW == 2 && warp >= 16));
     if constexpr (C::NWARPS == 20) {
         if (epi_warp) tc::setmaxnreg_inc<128>();
         else if (prod_warp) tc::setmaxnreg_dec<C::PROD_REGS>();
@@ -425,7 +454,7 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
         uint32_t stage = 0, phase = 0, rs = 0, rph = 0, seq = 0;
         bool ok = true;
         for (long long u = pair; u < units && ok; u += npairs) {
-            const Unit un = decode(a, u);
+            const Unit un = decode<C::XF>(a, u);
             if (un.skip) continue;
             for (int ks = 0; ks < nks; ++ks) {
                 if ((int)(seq++ % (uint32_t)PW) != pg) {
@@ -498,7 +527,7 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
         uint32_t accph[2] = {0u, 0u};
         int buf = 0;
         for (long long u = pair; u < units; u += npairs) {
-            Unit un = decode(a, u);
+            Unit un = decode<C::XF>(a, u);
             if (un.skip) continue;
             un.i0 += TI * (int)rank;  // this CTA's i-SNPs
             const int t = un.trait;
@@ -713,19 +742,22 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
             uint32_t as = 0, aph = 0, issued_a = 0;
             bool ok = true;
             for (long long u = pair; u < units && ok; u += npairs) {
-                const Unit un = decode(a, u);
+                const Unit un = decode<C::XF>(a, u);
                 if (un.skip) continue;
                 const int arow = 3 * (un.bd.start1 + un.i0 + TI * (int)rank);
+                const int xrow = ((un.trait * 2 + (int)rank) * a.nsnp + un.bd.start2 + un.j0) * 6;
                 for (int ks = 0; ks < nks; ++ks) {
                     if (!tc::mbar_wait(&sm.empty[as], aph ^ 1u, abort, a.wait_ns)) {
                         fail(a, sm, 7);
                         ok = false;
                         break;
                     }
-                    tc::mbar_arrive_expect_tx(&sm.full[as], A_BYTES);
+                    tc::mbar_arrive_expect_tx(&sm.full[as], C::XF ? A_BYTES + XB_BYTES : A_BYTES);
 #pragma unroll
                     for (int w = 0; w < 4; ++w)
                         tc::tma_load_2d(sm.a[as] + 32 * w * KS, &maps.hi, ks * KS, arow + A_BOX * w, &sm.full[as]);
+                    // the streamed-B variant: this CTA's half of the B stage, 126 expanded rows
+                    if constexpr (C::XF) tc::tma_load_2d(sm.b[as], &maps.hx, ks * KS, xrow, &sm.full[as]);
                     ++issued_a;
                     advance<STAGES>(as, aph);
                 }
@@ -741,7 +773,7 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
                 if (!tc::mbar_wait(&sm.full[slot], par, &no_abort, a.wait_ns)) fail(a, sm, 8);
             }
         }
-    } else if (warp == 14) {
+    } else if (warp == 14 && !C::XF) {
         // ---------------- raw loader: j one-hot rows and trait digit rows ----------------
         // gated only by the B producers' consumption, so it runs up to RSTAGES stages ahead
         // of them (the j rows come from DRAM once per pair tile)
@@ -749,7 +781,7 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
             uint32_t rs = 0, rph = 0, issued_r = 0;
             bool ok = true;
             for (long long u = pair; u < units && ok; u += npairs) {
-                const Unit un = decode(a, u);
+                const Unit un = decode<C::XF>(a, u);
                 if (un.skip) continue;
                 for (int ks = 0; ks < nks; ++ks) {
                     if (!tc::mbar_wait(&sm.raw_empty[rs], rph ^ 1u, abort, a.wait_ns)) {
@@ -777,7 +809,7 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
         uint32_t as = 0, aph = 0;
         bool ok = true;
         for (long long u = pair; u < units && ok; u += npairs) {
-            const Unit un = decode(a, u);
+            const Unit un = decode<C::XF>(a, u);
             if (un.skip) continue;
             for (int ks = 0; ks < nks; ++ks) {
                 if (!tc::mbar_wait(&sm.full[as], aph, abort, a.wait_ns)) {
@@ -801,7 +833,7 @@ __global__ void __launch_bounds__(C::NTHREADS, 1) k_scan_mma(ScanArgs a, const _
             ok = false;
         }
         for (long long u = pair; u < units && ok; u += npairs) {
-            const Unit un = decode(a, u);
+            const Unit un = decode<C::XF>(a, u);
             if (un.skip) continue;
             if (!tc::mbar_wait_cluster(&sm.acc_empty[buf], accph[buf] ^ 1u, abort, a.wait_ns)) {
                 fail(a, sm, 4);
@@ -887,6 +919,13 @@ cudaError_t mma_encode_traits(MmaMaps *maps, const int8_t *ydig, int ntraits, in
     return encode_2d(&maps->dg, ydig, (uint64_t)Np, (uint64_t)mma::ND * ntraits, mma::ND);
 }
 
+// The streamed-B variant's expanded rows [ntraits][2][nsnp][6][Np], in boxes of one CTA half
+// of a j tile (21 SNPs x 6 types = 126 rows)
+cudaError_t mma_encode_x(MmaMaps *maps, const int8_t *x, int nsnp, int Np, int ntraits)
+{
+    return encode_2d(&maps->hx, x, (uint64_t)Np, 12 * (uint64_t)nsnp * ntraits, 6 * mma::TJ);
+}
+
 bool mma_available() { return true; }
 int mma_tile_i() { return mma::TIP; }  // the host tiles blocks by CTA-pair tiles
 int mma_tile_j() { return mma::TJ; }
@@ -898,12 +937,16 @@ int mma_stage_individuals() { return mma::KS; }
 // of shared memory) and epilogue warps per TMEM lane quarter:
 //   0  6 slots / 6 raw, 2 epilogue warps   1  5 / 10, 2   2  6 / 4, 2   3  6 / 6, 3
 //   4  6 / 6, 2 epilogue warps, two producer groups on alternate stages
+//   5  6 slots, streamed B (expanded rows TMA-loaded from HBM; no producers, no raw ring)
 using Rings0 = mma::Rings<6, 6>;
 using Rings1 = mma::Rings<5, 10>;
 using Rings2 = mma::Rings<6, 4>;
 using Rings3 = mma::Rings<6, 6, 3>;
 using Rings4 = mma::Rings<6, 6, 2, 2>;
-constexpr int MMA_SHAPES = 5;
+using Rings5 = mma::Rings<6, 1, 2, 1, true>;
+constexpr int MMA_SHAPES = 6;
+
+bool mma_needs_x(int v) { return v == 5; }
 
 int mma_shapes() { return MMA_SHAPES; }
 
@@ -913,7 +956,8 @@ void mma_shape(int v, const char **desc)
                                             "5 operand slots / 10 raw stages, 8 epilogue warps",
                                             "6 operand slots / 4 raw stages, 8 epilogue warps",
                                             "6 operand slots / 6 raw stages, 12 epilogue warps (setmaxnreg)",
-                                            "6 operand slots / 6 raw stages, 8 epilogue warps, 2 producer groups (setmaxnreg)"};
+                                            "6 operand slots / 6 raw stages, 8 epilogue warps, 2 producer groups (setmaxnreg)",
+                                            "6 operand slots, B streamed from HBM, 8 epilogue warps"};
     if (desc) *desc = names[v];
 }
 
@@ -998,6 +1042,7 @@ cudaError_t mma_prepare(int v, int ntraits, int grid_request, int *grid)
     case 2: return prepare<Rings2>(v, ntraits, grid_request, grid);
     case 3: return prepare<Rings3>(v, ntraits, grid_request, grid);
     case 4: return prepare<Rings4>(v, ntraits, grid_request, grid);
+    case 5: return prepare<Rings5>(v, ntraits, grid_request, grid);
     }
     return cudaErrorInvalidValue;
 }
@@ -1011,6 +1056,7 @@ cudaError_t mma_enqueue(int v, const ScanArgs &a, const MmaMaps &maps, int grid,
     case 2: return enqueue<Rings2>(a, maps, grid, stream);
     case 3: return enqueue<Rings3>(a, maps, grid, stream);
     case 4: return enqueue<Rings4>(a, maps, grid, stream);
+    case 5: return enqueue<Rings5>(a, maps, grid, stream);
     }
     return cudaErrorInvalidValue;
 }

@@ -2,7 +2,8 @@
 
 Each form has a table of kernel variants (plain form: tile shapes -- 64 x 64 with 8 pairs per
 thread, 64 x 32 with 4, 32 x 128 with 8; tensor form: operand ring depths, 8 or 12
-epilogue warps, one or two producer groups). Every variant must
+epilogue warps, one or two producer groups, B built in shared memory or streamed from HBM).
+Every variant must
 give the oracle's results: counts and df exact, F within the parity bar, the same hits in the
 same order (several uneven chromosome blocks, several traits with their own masks). The
 autotuner times every candidate once per device, form, individual count and trait count and
@@ -18,7 +19,7 @@ pytestmark = pytest.mark.gpu
 
 F_TOL = 1e-5
 TOL_SET = 1e-4
-N_CANDIDATES = {capi.FORM_POPC: 3, capi.FORM_TENSOR: 5}
+N_CANDIDATES = {capi.FORM_POPC: 3, capi.FORM_TENSOR: 6}
 VARIANTS = [(f, c) for f in (capi.FORM_POPC, capi.FORM_TENSOR) for c in range(1, N_CANDIDATES[f] + 1)]
 
 
