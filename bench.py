@@ -468,6 +468,9 @@ def main():
                     "peak_source": "2 x dense bf16 of MEASURED_PEAKS.json (%s, %.1f TFLOP/s burst)"
                                    % (peak_kind, peaks["bf16_tflops"]),
                     "cublas_int8_same_run": int8, "frac_of_cublas_int8_same_run": achieved / int8,
+                    # the same against the sustained (power-capped) bf16 figure of the file
+                    "frac_of_2x_sustained_bf16": (achieved / (2.0 * peaks["bf16_tflops_sustained"])
+                                                  if peaks.get("bf16_tflops_sustained") else None),
                     "traffic": traffic, "traffic_unit": "bytes per launch",
                     "traffic_source": "ncu dram__bytes_read+write on cfg3m, scaled by pairs x individuals"}
         else:
