@@ -842,6 +842,14 @@ epi_status pick_variant(epi_ctx *ctx, const epi_scan_opts *o, int form, int *v, 
                                     : snprintf(buf + len, sizeof(buf) - len, "%s n/a", c ? " /" : "");
     *v = best;
     *how = buf;
+    // the streamed-B candidate's expanded rows (up to 32 GiB) are released when it lost
+    if (form == EPI_FORM_TENSOR && !epi::mma_needs_x(best) && ctx->d_x) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->d_x);
+        ctx->d_x = nullptr;
+        ctx->x_cap = 0;
+        ctx->x_valid = false;
+    }
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tune.push_back({ctx->device, form, ctx->Np, ctx->ntraits, best, *how});
     return EPI_OK;
