@@ -270,6 +270,67 @@ def cpu_baseline(data, test, t1, t2, budget_s=12.0, min_m=200):
                                                                                          else "8df", dt)}
 
 
+DATAMODE_METRIC = "PLINK .ped/.map -> .epigpu conversion (epiGPU -Dr), MB of .ped text per second"
+
+
+def run_datamode(args):
+    """The data mode beside the scan (host C, one thread): `epiGPU -Dr` converting a seeded
+    PLINK fileset of 2,000 individuals x 5,000 SNPs (40 MB of .ped text) to .epigpu, K timed runs
+    after W warm-up runs; with --impl reference the reference's own readplink.c functions
+    (oracle/_ref/plinkref, built from its sources) on the same files. The two outputs are
+    compared byte for byte."""
+    import tempfile
+    from epigpu_b200 import synth
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    cli = ROOT / "epigpu_b200" / "bin" / "epiGPU"
+    ref = ROOT / "oracle" / "_ref" / "plinkref"
+    reference = args.impl == "reference"
+    exe = ref if reference else cli
+    if not exe.exists():
+        print(json.dumps({"impl": args.impl, "unavailable": "%s is not built" % exe.relative_to(ROOT)}))
+        return 0
+    nid, nsnp = 2000, 5000
+    with tempfile.TemporaryDirectory() as tmp:
+        d = pathlib.Path(tmp)
+        ped, mp = synth.write_plink_fileset(d, nid, nsnp, seed=1)
+        mb = ped.stat().st_size / 1e6
+        out = d / "out.epigpu"
+        cmd = [str(ref), "write", str(ped), str(mp), str(out)] if reference else [str(cli), "-Dr", str(ped), str(mp),
+                                                                                  str(out)]
+        times = []
+        for step in range(args.warmup + args.steps):
+            t = time.perf_counter()
+            subprocess.run(cmd, check=True, capture_output=True)
+            if step >= args.warmup:
+                times.append(time.perf_counter() - t)
+        same = None
+        other = cli if reference else ref
+        if other.exists():
+            cmp = d / "other.epigpu"
+            ocmd = [str(cli), "-Dr", str(ped), str(mp), str(cmp)] if reference else [str(ref), "write", str(ped),
+                                                                                      str(mp), str(cmp)]
+            subprocess.run(ocmd, check=True, capture_output=True)
+            same = out.read_bytes() == cmp.read_bytes()
+    value = mb * len(times) / sum(times)
+    line = {
+        "metric": DATAMODE_METRIC, "value": value, "unit": "MB/s", "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "none", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "datamode: PLINK text %d individuals x %d SNPs (%.1f MB .ped)" % (nid, nsnp, mb),
+                   "identical_to_other_arm": same},
+        "e2e": {"value": value, "unit": "MB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "roofline": None, "cpu_baseline": None,
+    }
+    if reference:
+        line["impl"] = "reference"
+        line["cpu_baseline"] = {"value": value, "unit": "MB/s", "cores": 1, "kind": "reference",
+                                "sample": "the reference's dims/readped/readmap/pack/createpackedbinary on the fileset"}
+    print(json.dumps(line))
+    return 0
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -331,7 +392,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS) + ["datamode"],
+                    help="a scan configuration, or `datamode`: the host's PLINK -> .epigpu conversion")
     ap.add_argument("--form", default="auto", choices=["auto", "popc", "tensor"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile", type=int, default=0,
@@ -344,6 +406,8 @@ def main():
                     help="side of the square block whose pairs' F error against the FP64 oracle is reported "
                          "(0 = none)")
     args = ap.parse_args()
+    if args.workload == "datamode":
+        return run_datamode(args)
     if args.impl == "reference":
         return run_reference(args)
 

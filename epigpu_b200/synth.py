@@ -153,3 +153,37 @@ def packed_on_gpu(nid, nsnp, seed, miss=0.01, chunk=4096):
         w = torch.where(w >= 2 ** 31, w - 2 ** 32, w).to(torch.int32)
         out[s0:s0 + m].copy_(w.cpu())
     return out.numpy()
+
+
+def write_plink_fileset(directory, nid, nsnp, seed, nchr=4):
+    """A seeded PLINK text fileset (`x.ped`, `x.map`) for timing the data mode: per SNP two of
+    A/C/G/T; genotypes among both homozygotes, both heterozygote orders and missing (0 0);
+    individual 0 homozygous and individual 1 heterozygous at every SNP (the reference's reader
+    needs a homozygote to code the alleles); a normal trait with every seventh value -9;
+    SNPs on `nchr` chromosomes in order. Built with array operations (a 2,000 x 5,000 fileset,
+    40 MB of .ped text, in about a second)."""
+    import pathlib
+    d = pathlib.Path(directory)
+    rng = np.random.default_rng(seed)
+    letters = np.frombuffer(b"ACGT", np.uint8)
+    al = np.argsort(rng.random((nsnp, 4)), axis=1)[:, :2]
+    a, b = letters[al[:, 0]], letters[al[:, 1]]
+    g = rng.choice(5, (nid, nsnp), p=[0.35, 0.15, 0.15, 0.3, 0.05])
+    g[0, :] = 0
+    g[min(1, nid - 1), :] = 1
+    zero = np.uint8(ord("0"))
+    first = np.select([g == 0, g == 1, g == 2, g == 3], [a, a, b, b], zero).astype(np.uint8)
+    second = np.select([g == 0, g == 1, g == 2, g == 3], [a, b, a, b], zero).astype(np.uint8)
+    row = np.empty((nid, nsnp, 4), np.uint8)
+    row[..., 0], row[..., 1], row[..., 2], row[..., 3] = first, 32, second, 32
+    row[:, -1, 3] = 10
+    y = rng.standard_normal(nid)
+    with open(d / "x.ped", "wb") as f:
+        for i in range(nid):
+            phen = "-9" if i % 7 == 3 else "%.6f" % y[i]
+            f.write(("F%d ind%d 0 pat%d %d %s " % (i // 3, i, i, 1 + i % 2, phen)).encode())
+            f.write(row[i].tobytes())
+    chrs = np.sort(rng.integers(1, nchr + 1, nsnp))
+    with open(d / "x.map", "w") as f:
+        f.write("".join("chr%d rs%d %.4f %d\n" % (c, 1000 + j, 0.01 * j, 5000 + 37 * j) for j, c in enumerate(chrs)))
+    return d / "x.ped", d / "x.map"

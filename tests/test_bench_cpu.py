@@ -77,3 +77,20 @@ def test_max_over_ranks_single_process():
     sys.path.insert(0, str(ROOT))
     import bench
     assert bench.max_over_ranks(3.25, None) == 3.25
+
+
+@pytest.mark.skipif(not (ROOT / "epigpu_b200" / "bin" / "epiGPU").exists() or
+                    not (ROOT / "oracle" / "_ref" / "plinkref").exists(),
+                    reason="host program or the reference's data-mode oracle not built")
+@pytest.mark.parametrize("impl", ["ours", "reference"])
+def test_datamode_workload(impl):
+    """The data-mode measurement (PLINK text -> .epigpu on the host): one JSON line per arm, and
+    the two arms' .epigpu files byte-identical."""
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--workload", "datamode", "--impl", impl,
+                        "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=300, cwd=str(ROOT))
+    assert r.returncode == 0, r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["unit"] == "MB/s" and d["value"] > 0 and d["config"]["identical_to_other_arm"] is True
+    assert (d.get("impl") == "reference") == (impl == "reference")
