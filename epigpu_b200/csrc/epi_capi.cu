@@ -781,8 +781,11 @@ epi_status pick_variant(epi_ctx *ctx, const epi_scan_opts *o, int form, int *v, 
     }
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
+        // (a kept choice of the streamed-B variant holds only while this context's expanded rows
+        // would fit: another context of the same shape may hold more SNPs)
         for (const TuneEntry &t : g_tune)
-            if (t.device == ctx->device && t.form == form && t.Np == ctx->Np && t.ntraits == ctx->ntraits) {
+            if (t.device == ctx->device && t.form == form && t.Np == ctx->Np && t.ntraits == ctx->ntraits &&
+                !(form == EPI_FORM_TENSOR && epi::mma_needs_x(t.variant) && !x_candidate(ctx))) {
                 *v = t.variant;
                 *how = t.how;
                 return EPI_OK;
