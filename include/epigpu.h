@@ -193,7 +193,8 @@ epi_status epi_get_stream(const epi_ctx *ctx, void **stream);
  * Working memory is a fixed array of about 520 KiB in this library, one per device, held
  * until the process exits: it limits nid to EPI_NOALLOC_MAX_NID (larger returns
  * EPI_E_UNSUPPORTED). The first call on each device does that device's set-up (device
- * check, SM count, kernel attribute); make that first call before any CUDA stream capture.
+ * check, SM count, kernel attribute). No call may be made while `stream` is being captured
+ * into a CUDA graph: every call copies the hit count to the host and synchronises.
  * Every call looks up the array's device address for the current device. All calls on a
  * device share the array and each call clears what it needs, so results never carry over,
  * but calls that overlap on the GPU (other host threads, other streams) race and must be
