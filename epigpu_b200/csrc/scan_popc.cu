@@ -9,13 +9,15 @@
 // arrive by TMA, 64 individuals per stage, in a three-stage ring. Each SNP's two genotypes
 // other than its most frequent one are its dense genotypes A and B. Per stage:
 //   * expansion (all threads, double-buffered): for each i-SNP, U_A = [g_i==A]*y and
-//     U_B = [g_i==B]*y floats in shared memory, with the phenotype-masked plane words of A, B
-//     and of the missing calls;
+//     U_B = [g_i==B]*y floats in shared memory, two i-SNPs side by side, with the
+//     phenotype-masked plane words of A, B and of the missing calls;
 //   * cell counts of the dense 2x2 cells and of the individuals missing at j: AND + __popc of
 //     32-bit plane words, 16-bit packed counters;
 //   * cell sums S_{Ai,Aj}, S_{Ai,Bj}, S_{Bi,Aj}, S_{Bi,Bj}: each lane holds its own j-SNP's
 //     plane words and adds the warp's broadcast U values into the cells its genotype bits
-//     select (4 FP32 adds per pair and individual, predicated by the bits);
+//     select (4 FP32 adds per pair and individual, predicated by the bits; the bit of the
+//     lane's j-SNP is the same for two i-SNPs, so each predicated instruction is a packed
+//     f32x2 add serving two pairs, rounded like two scalar adds);
 //   * individuals missing at the j-SNP (per lane, sparse): their sums by the i genotype;
 //   * individuals missing at the i-SNP (warp-uniform, sparse): their sums and counts by the
 //     j genotype, and the sum of y^2 of individuals missing at both SNPs.
@@ -47,15 +49,15 @@ struct Shape {
     static constexpr int NT = WI * WJ * 32;   // threads
     static constexpr int KW = 2;              // 32-individual words per stage
     static constexpr int KI = 32 * KW;        // individuals per stage
-    static constexpr int KP = KI / 2;         // individual pairs per stage
     static constexpr int RS = 3;              // TMA ring depth
     static constexpr uint32_t STAGE_BYTES = (TI + TJ) * KW * 16;  // transaction bytes per stage
     static_assert(TI * KW <= NT - KI / 4 && TI <= 256 && TJ <= 256 && TI + TJ <= NT, "expansion roles");
+    static_assert(PI % 2 == 0, "i-SNPs in pairs (packed FP32 adds)");
 
     struct Smem {
         uint4 raw_i[RS][TI][KW];  // TMA: plane words of the i-tile (row = SNP)
         uint4 raw_j[RS][TJ][KW];  // TMA: plane words of the j-tile
-        float4 u[2][KP][TI];      // (U_A(k), U_A(k+1), U_B(k), U_B(k+1)) of each i-SNP
+        float4 u[2][KI][TI / 2];  // (U_A, U_A', U_B, U_B') of i-SNPs 2p, 2p + 1 at individual k
         uint4 pm[2][KW][TI];      // (P_A & W, P_B & W, missing & W, W) of each i-SNP
         float y[2][KI];           // the stage's trait values (0 where invalid)
         float4 sps[PI][NT];       // per pair: sums over individuals missing at i by g_j: S_30..S_32, QMM
@@ -213,24 +215,24 @@ __global__ void __launch_bounds__(Sh::NT, 1) k_scan_popc(ScanArgs a, const __gri
             for (int st = 0; st < min(RS, nst); ++st) issue(st);
         __syncthreads();  // maj
 
-        // expansion of stage st into buffer b: work item -> (i-SNP, 8 individuals), consecutive
-        // threads on consecutive i-SNPs (contiguous stores, the same trait words in a warp)
+        // expansion of stage st into buffer b: work item -> (pair of i-SNPs, 4 individuals),
+        // consecutive threads on consecutive i-SNP pairs (contiguous stores, the same trait
+        // words in a warp)
         auto expand = [&](int st, int b) {
             const int r = st % RS;
             for (int it = tid; it < 8 * TI; it += NT) {
-                const int i = it % TI, part = it / TI, w = part >> 2, k8 = 8 * (part & 3);
-                const uint4 P = sm.raw_i[r][i][w];
-                const int mj = sm.maj[i];
-                const uint32_t PA = mj == 0 ? P.y : P.x, PB = mj == 2 ? P.y : P.z;
-                const float4 ya = __ldg(reinterpret_cast<const float4 *>(yt + KI * st + 32 * w + k8));
-                const float4 yb = __ldg(reinterpret_cast<const float4 *>(yt + KI * st + 32 * w + k8 + 4));
-                const float yv[8] = {ya.x, ya.y, ya.z, ya.w, yb.x, yb.y, yb.z, yb.w};
+                const int p = it % (TI / 2), part = it / (TI / 2), w = part >> 3, k4 = 4 * (part & 7);
+                const uint4 P0 = sm.raw_i[r][2 * p][w], P1 = sm.raw_i[r][2 * p + 1][w];
+                const int m0 = sm.maj[2 * p], m1 = sm.maj[2 * p + 1];
+                const uint32_t PA0 = m0 == 0 ? P0.y : P0.x, PB0 = m0 == 2 ? P0.y : P0.z;
+                const uint32_t PA1 = m1 == 0 ? P1.y : P1.x, PB1 = m1 == 2 ? P1.y : P1.z;
+                const float4 y4 = __ldg(reinterpret_cast<const float4 *>(yt + KI * st + 32 * w + k4));
+                const float yv[4] = {y4.x, y4.y, y4.z, y4.w};
 #pragma unroll
-                for (int e = 0; e < 8; e += 2) {
-                    const int k = k8 + e;
-                    sm.u[b][16 * w + k / 2][i] =
-                        make_float4(bit(PA, k) ? yv[e] : 0.f, bit(PA, k + 1) ? yv[e + 1] : 0.f,
-                                    bit(PB, k) ? yv[e] : 0.f, bit(PB, k + 1) ? yv[e + 1] : 0.f);
+                for (int e = 0; e < 4; ++e) {
+                    const int k = k4 + e;
+                    sm.u[b][32 * w + k][p] = make_float4(bit(PA0, k) ? yv[e] : 0.f, bit(PA1, k) ? yv[e] : 0.f,
+                                                         bit(PB0, k) ? yv[e] : 0.f, bit(PB1, k) ? yv[e] : 0.f);
                 }
             }
             if (tid < TI * KW) {
@@ -250,12 +252,13 @@ __global__ void __launch_bounds__(Sh::NT, 1) k_scan_popc(ScanArgs a, const __gri
         expand(0, 0);
         __syncthreads();
 
-        float S[PI][4];
+        float2 S[PI / 2][4];  // the cell sums of i-SNPs ib + 2p (x) and ib + 2p + 1 (y)
         uint32_t C[PI][3];
 #pragma unroll
         for (int ii = 0; ii < PI; ++ii) {
+            if (ii % 2 == 0)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) S[ii][c] = 0.f;
+                for (int c = 0; c < 4; ++c) S[ii / 2][c] = make_float2(0.f, 0.f);
             C[ii][0] = C[ii][1] = C[ii][2] = 0u;
         }
         const int mjj = sm.majj[jl];  // this lane's j-SNP: its dense genotypes' planes
@@ -311,22 +314,19 @@ __global__ void __launch_bounds__(Sh::NT, 1) k_scan_popc(ScanArgs a, const __gri
                         sm.spj[ii][tid] = acc;
                     }
                 }
-                // sums: this lane's j genotype bits select the cells the U values go to
+                // sums: this lane's j genotype bit of individual k selects the cells the U
+                // values go to; one packed FP32 add serves two i-SNPs (the same j bit)
 #pragma unroll
-                for (int h = 0; h < 16; ++h) {
-                    const int k = 2 * h;
-                    const bool fAa = bit(PAj, k), fBa = bit(PBj, k), fAb = bit(PAj, k + 1), fBb = bit(PBj, k + 1);
+                for (int k = 0; k < 32; ++k) {
+                    const bool fA = bit(PAj, k), fB = bit(PBj, k);
 #pragma unroll
-                    for (int ii = 0; ii < PI; ++ii) {
-                        const float4 uu = sm.u[b][16 * w + h][ib + ii];
-                        if (fAa) S[ii][0] += uu.x;
-                        if (fBa) S[ii][1] += uu.x;
-                        if (fAa) S[ii][2] += uu.z;
-                        if (fBa) S[ii][3] += uu.z;
-                        if (fAb) S[ii][0] += uu.y;
-                        if (fBb) S[ii][1] += uu.y;
-                        if (fAb) S[ii][2] += uu.w;
-                        if (fBb) S[ii][3] += uu.w;
+                    for (int q = 0; q < PI / 2; ++q) {
+                        const float4 uu = sm.u[b][32 * w + k][ib / 2 + q];
+                        const float2 ua = make_float2(uu.x, uu.y), ub = make_float2(uu.z, uu.w);
+                        if (fA) S[q][0] = __fadd2_rn(S[q][0], ua);
+                        if (fB) S[q][1] = __fadd2_rn(S[q][1], ua);
+                        if (fA) S[q][2] = __fadd2_rn(S[q][2], ub);
+                        if (fB) S[q][3] = __fadd2_rn(S[q][3], ub);
                     }
                 }
             }
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(Sh::NT, 1) k_scan_popc(ScanArgs a, const __gri
             if (valid) {
                 PairIn p;
 #pragma unroll
-                for (int c = 0; c < 4; ++c) p.S[c] = S[ii][c];
+                for (int c = 0; c < 4; ++c) p.S[c] = ii % 2 ? S[ii / 2][c].y : S[ii / 2][c].x;
                 const float2 sj = sm.spj[ii][tid];
                 p.SJ[0] = sj.x;
                 p.SJ[1] = sj.y;

@@ -78,10 +78,12 @@ typedef struct epi_scan_opts {
                             * the same scan shape (kernel arguments, blocks) replays it with one
                             * launch; 1: every operation is launched directly */
     int32_t tile_config;   /* 0: the kernel variant (plain form: tile shape, 3 candidates;
-                            * tensor form: ring depths, epilogue warps and producer groups, 5
-                            * candidates) is chosen by the autotuner, which times every candidate
-                            * on a sample block once per device, form, individual count and
-                            * trait count; k >= 1: candidate k (epi_scan_config names it) */
+                            * tensor form: ring depths, epilogue warps, producer groups and
+                            * streamed B, 6 candidates, streamed B only up to 6,144 padded
+                            * individuals) is chosen by the autotuner, which times every
+                            * candidate on a sample block once per device, form, individual
+                            * count and trait count; k >= 1: candidate k (epi_scan_config
+                            * names it) */
     int32_t reserved[5];   /* set to 0 */
 } epi_scan_opts;
 
