@@ -520,7 +520,7 @@ epi_status setup_run(epi_ctx *ctx, const epi_block *blocks, int nblocks, const e
     r.form = pick_form(ctx, o);
     r.variant = variant;
     if (r.form == EPI_FORM_TENSOR && !epi::mma_available())
-        return set_err(ctx, EPI_E_UNSUPPORTED, "tensor form not available in this build");
+        return set_err(ctx, EPI_E_UNSUPPORTED, "tensor form not available in this library");
     if (r.form == EPI_FORM_TENSOR && ctx->Np > epi::mma_max_nid())
         return set_err(ctx, EPI_E_UNSUPPORTED, "tensor form: at most %d individuals", epi::mma_max_nid());
     if (r.form == EPI_FORM_POPC && ctx->nid > 65535)

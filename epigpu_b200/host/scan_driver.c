@@ -32,7 +32,7 @@
 
 #define PAIR_BATCH ((long long)1 << 34) /* pairs per launch batch between checkpoints */
 
-/* Settings this build adds to the reference's globals (src/epiopencl.h:9-16, which the
+/* Settings this scan driver adds to the reference's globals (src/epiopencl.h:9-16, which the
  * caller's main.c defines). They are defined here, with their defaults, so that the
  * reference's own main.c links against this file unchanged: the GPU form (-g), the
  * permutation-threshold count (-N) and the reference's resume rule (-R). */
@@ -43,7 +43,7 @@ int UREFRESUME = 0;
 static void fail(epi_ctx *ctx, epi_status st, const char *what)
 {
     if (st == EPI_E_NODEVICE) {
-        printf("\n\nError:\nThere is no suitable GPU on this computer.\nThis build requires an NVIDIA B200 "
+        printf("\n\nError:\nThere is no suitable GPU on this computer.\nThis program requires an NVIDIA B200 "
                "(sm_100a) device; -d selects it.\n\n");
         exit(1);
     }

@@ -1,12 +1,12 @@
-"""The drop-in recipe for the reference's own build (INTEGRATION.md, section 1): epiGPU's
+"""The drop-in recipe for the reference's own build: epiGPU's
 src/main.c, src/readplink.c and src/timing.c, compiled unmodified, with src/EpiOpenCL.c
-replaced by this build's perform_scan (epigpu_b200/host/scan_driver.c, the reference's
+replaced by epigpu_b200's perform_scan (epigpu_b200/host/scan_driver.c, the reference's
 signature and globals, src/epiopencl.h:9-21) and -lOpenCL by libepigpu.so. The recipe is the
 `refmain` target of oracle/Makefile, which writes oracle/_ref/epiGPU_refmain.
 
 CPU: the recipe builds from the reference tree, and the binary runs the reference's own CLI
 paths that need no GPU (usage text, argument checks, a clean "no suitable GPU" exit).
-GPU: its `-A` results file is byte-identical to this build's own epiGPU program on the same
+GPU: its `-A` results file is byte-identical to epigpu_b200's own epiGPU program on the same
 data and options, with and without the reference's permutation (-p), 8 df and 4 df."""
 import os
 import pathlib
@@ -39,7 +39,7 @@ def test_recipe_links_reference_sources_to_the_library():
         assert r.returncode == 0, r.stdout + r.stderr
     syms = subprocess.run(["nm", str(REFMAIN)], capture_output=True, text=True).stdout
     defined = {ln.split()[-1] for ln in syms.splitlines() if len(ln.split()) == 3 and ln.split()[1] in "TtBbDdCc"}
-    # the reference's CLI and loader, this build's scan driver; no OpenCL left
+    # the reference's CLI and loader, epigpu_b200's scan driver; no OpenCL left
     for name in ("main", "analysismodecl", "readpackedbinary", "permute", "perform_scan", "resume_point",
                  "UFORM", "UNPERM", "UREFRESUME"):
         assert name in defined, name
